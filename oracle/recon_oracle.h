@@ -1,0 +1,69 @@
+/* TEST INFRASTRUCTURE — NOT THE PRODUCT.
+ *
+ * CPU restatement of AreTomo3's reconstruction path (AreTomo/Recon) used as
+ * the checker for the CUDA implementation: the FP64 instantiation is the
+ * oracle every GPU result is measured against; the FP32 instantiation (same
+ * code, float arithmetic, OpenMP over y-slices) is the timed CPU baseline.
+ * Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg and
+ * reference arm load it.
+ *
+ * Parity pin: the functions below are checked against outputs of the
+ * reference's own CUDA Recon (compiled from the reference sources for sm_100a,
+ * oracle/ref/) stored as fixtures in tests/golden/.
+ *
+ * Conventions (all as in the reference):
+ *   nx, ny, T   projection width, height, tilt count; frames[T][ny][nx]
+ *   Nx = nx & ~1   volume width and the R-weight FFT length
+ *   Nz = volZ      volume thickness
+ *   output volume: vol[ny][Nz][Nx], frame y = XZ slice with z flipped
+ *   (AreTomo/Recon/CDoWbpRecon.cpp:107-123).
+ */
+#ifndef AT3R_RECON_ORACLE_H
+#define AT3R_RECON_ORACLE_H
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* How a complex-to-real inverse FFT treats imaginary parts in its DC and
+ * Nyquist bins (only reachable through the WBP Fourier crop, whose cropped
+ * spectrum is not Hermitian).  0: the real part of the Hermitian-extended
+ * inverse (imaginary DC/Nyquist parts dropped); 1: the half-length complex
+ * "packing" algorithm, in which they leak into even/odd samples. */
+void oracle_set_c2r_mode(int mode);
+int oracle_get_c2r_mode(void);
+
+/* Per-tilt cos/sin table as the reference builds it (CTomoBase.cpp:56-65). */
+void oracle_cos_sin(const float* tilts_deg, int n_tilts, float* cos_sin);
+
+/* WBP of y-slices [y0, y1).  out: [(y1-y0)][Nz][Nx], z flipped. */
+int oracle_wbp_f64(const float* frames, int nx, int ny, int n_tilts, const float* tilts_deg,
+                   int vol_z, int y0, int y1, double* out, int n_threads);
+int oracle_wbp_f32(const float* frames, int nx, int ny, int n_tilts, const float* tilts_deg,
+                   int vol_z, int y0, int y1, float* out, int n_threads);
+
+/* SART of y-slices [y0, y1).  relax <= 0 selects the reference's 1/subsets.
+ * rfactor (may be NULL): per-iteration sum|raw - fp| and sum|raw| over the
+ * valid detector samples of every subset, as 2*iters doubles. */
+int oracle_sart_f64(const float* frames, int nx, int ny, int n_tilts, const float* tilts_deg,
+                    int vol_z, int start_tilt, int num_tilts, int iters, int subsets, double relax,
+                    int y0, int y1, double* out, double* rfactor, int n_threads);
+int oracle_sart_f32(const float* frames, int nx, int ny, int n_tilts, const float* tilts_deg,
+                    int vol_z, int start_tilt, int num_tilts, int iters, int subsets, double relax,
+                    int y0, int y1, float* out, double* rfactor, int n_threads);
+
+/* Components, for known-answer tests. */
+/* complex FFT of length n, interleaved re/im; sign -1 forward, +1 inverse, unnormalised */
+int oracle_fft_f64(const double* in, int n, int sign, double* out);
+/* the R-weight filter of one row of length N (even): R2C, x H(k), C2R */
+int oracle_rweight_row_f64(const double* in, int n, double* out);
+/* the filter's transfer function H(k), k in [0, N/2] */
+void oracle_rweight_filter_f64(int n, double* h);
+/* 2x grid -> 1x Fourier crop: g[2Nz][2Nx] -> f[Nz][Nx] (not flipped) */
+int oracle_fourier_crop_f64(const double* g, int nx_vol, int nz_vol, double* f);
+/* inverse real FFT of length n from n/2+1 bins under the current c2r mode */
+int oracle_c2r_f64(const double* in_cplx, int n, double* out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,39 @@
+#!/usr/bin/env bash
+# Test infrastructure only: compiles the reference's own CUDA Recon
+# (AreTomo3 AreTomo/Recon + the MaUtil/DataUtil/MrcUtil files it needs) for
+# sm_100a from the reference sources where they lie, plus this directory's
+# driver and stub, into oracle/_ref/ref_recon.  Nothing is copied out of the
+# reference tree; objects go to oracle/_ref/obj.
+set -euo pipefail
+REF=${AT3R_REFERENCE:-/root/reference}
+HERE=$(cd "$(dirname "$0")" && pwd)
+OUT="$HERE/../_ref"
+OBJ="$OUT/obj"
+mkdir -p "$OBJ"
+[ -d "$REF/AreTomo/Recon" ] || { echo "reference tree not found at $REF" >&2; exit 1; }
+NVCC=${NVCC:-nvcc}
+CUFLAGS="-std=c++17 -O2 -Xptxas -dlcm=ca -gencode arch=compute_100a,code=sm_100a -I$REF/LibSrc/Include -I$REF"
+CXXFLAGS="-std=c++17 -O2 -pthread -m64 -I$REF/LibSrc/Include -I$REF -I/usr/local/cuda/include"
+CU="AreTomo/Recon/GBackProj AreTomo/Recon/GBackProjWbp AreTomo/Recon/GDiffProj AreTomo/Recon/GForProj
+    AreTomo/Recon/GRWeight AreTomo/Recon/GWeightProjs AreTomo/Recon/GCalcRFactor
+    MaUtil/GFFT1D MaUtil/GFillEmpty2D MaUtil/GGenRandoms MaUtil/GFourierResize2D MaUtil/GFFTUtil2D"
+CPP="AreTomo/Recon/CTomoBase AreTomo/Recon/CTomoWbp AreTomo/Recon/CTomoSart AreTomo/Recon/CDoBaseRecon
+     AreTomo/Recon/CDoWbpRecon AreTomo/Recon/CDoSartRecon MaUtil/CCufft2D MaUtil/CPad2D MaUtil/CSimpleFuncs
+     AreTomo/Util/CSplitItems DataUtil/CTiltSeries DataUtil/CMrcStack AreTomo/MrcUtil/CAlignParam
+     AreTomo/MrcUtil/CDarkFrames LibSrc/Mrcfile/Image/C4BitImage LibSrc/Util/Util_Time"
+objs=()
+for f in $CU; do
+  o="$OBJ/$(echo "$f" | tr / _).o"
+  [ "$o" -nt "$REF/$f.cu" ] || $NVCC $CUFLAGS -c "$REF/$f.cu" -o "$o"
+  objs+=("$o")
+done
+for f in $CPP; do
+  o="$OBJ/$(echo "$f" | tr / _).o"
+  [ "$o" -nt "$REF/$f.cpp" ] || g++ $CXXFLAGS -c "$REF/$f.cpp" -o "$o"
+  objs+=("$o")
+done
+g++ $CXXFLAGS -c "$HERE/ref_stub.cpp" -o "$OBJ/ref_stub.o"
+g++ $CXXFLAGS -c "$HERE/ref_driver.cpp" -o "$OBJ/ref_driver.o"
+$NVCC -gencode arch=compute_100a,code=sm_100a -o "$OUT/ref_recon" "${objs[@]}" \
+  "$OBJ/ref_stub.o" "$OBJ/ref_driver.o" -lcufft -lcurand -lcuda
+echo "built $OUT/ref_recon"
