@@ -1,0 +1,611 @@
+// C-ABI implementation: plans, workspace, the y-slab loop and the host-buffer
+// path.  Declarations and data layouts: include/at3r.h.
+#include "at3r.h"
+#include "recon_kernels.cuh"
+
+#include <cuda_runtime.h>
+#include <dlfcn.h>
+
+#include <algorithm>
+#include <cmath>
+#include <complex>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <string>
+#include <vector>
+
+using namespace at3r;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+at3r_status set_err(at3r_status s, const std::string& msg)
+{
+    g_last_error = msg;
+    return s;
+}
+
+#define AT3R_CUDA(call)                                                                        \
+    do {                                                                                       \
+        cudaError_t e_ = (call);                                                               \
+        if (e_ != cudaSuccess)                                                                 \
+            return set_err(e_ == cudaErrorMemoryAllocation ? AT3R_ERR_OUT_OF_MEMORY : AT3R_ERR_CUDA, \
+                           std::string(#call) + ": " + cudaGetErrorString(e_));                \
+    } while (0)
+
+// ---------------------------------------------------------------------------
+// FFT planning: factor n into radices {8, 4, 2, 3, 5, 7, 11, 13}; any other
+// prime factor sends the length through Bluestein on m = 2^k >= 2n - 1.
+// ---------------------------------------------------------------------------
+bool factor_direct(int n, std::vector<int>& rad)
+{
+    rad.clear();
+    int m = n;
+    while (m % 8 == 0) { rad.push_back(8); m /= 8; }
+    if (m % 4 == 0) { rad.push_back(4); m /= 4; }
+    if (m % 2 == 0) { rad.push_back(2); m /= 2; }
+    for (int p : {3, 5, 7, 11, 13})
+        while (m % p == 0) { rad.push_back(p); m /= p; }
+    if (n == 1) rad.push_back(1);
+    return m == 1 && (int)rad.size() <= kMaxFftStages;
+}
+
+struct HostFft {
+    FftPlan plan{};
+    float2* d_tables = nullptr;  // twiddles, chirp, bhat in one allocation
+    size_t bytes = 0;
+};
+
+void fill_twiddles(std::vector<float2>& v, int n)
+{
+    v.resize(n);
+    for (int k = 0; k < n; k++) {
+        const double a = -2.0 * M_PI * (double)k / (double)n;
+        v[k] = make_float2((float)std::cos(a), (float)std::sin(a));
+    }
+}
+
+// Reference FFT in double for the Bluestein kernel spectrum (host only).
+void host_fft_pow2(std::vector<std::complex<double>>& a, int sign)
+{
+    const int n = (int)a.size();
+    for (int i = 1, j = 0; i < n; i++) {
+        int bit = n >> 1;
+        for (; j & bit; bit >>= 1) j ^= bit;
+        j ^= bit;
+        if (i < j) std::swap(a[i], a[j]);
+    }
+    for (int len = 2; len <= n; len <<= 1) {
+        const double ang = sign * 2.0 * M_PI / len;
+        for (int i = 0; i < n; i += len)
+            for (int k = 0; k < len / 2; k++) {
+                std::complex<double> w(std::cos(ang * k), std::sin(ang * k));
+                auto u = a[i + k], v = a[i + k + len / 2] * w;
+                a[i + k] = u + v;
+                a[i + k + len / 2] = u - v;
+            }
+    }
+}
+
+at3r_status make_fft(int n, HostFft& h)
+{
+    std::vector<int> rad;
+    FftPlan& p = h.plan;
+    p.n = n;
+    std::vector<float2> tw, chirp, bhat;
+    if (factor_direct(n, rad)) {
+        p.bluestein = 0;
+        p.work = n;
+        p.d.n = n;
+        p.d.nst = (n == 1) ? 0 : (int)rad.size();
+        for (int i = 0; i < p.d.nst; i++) p.d.radix[i] = rad[i];
+        fill_twiddles(tw, n);
+    } else {
+        int m = 1;
+        while (m < 2 * n - 1) m <<= 1;
+        factor_direct(m, rad);
+        p.bluestein = 1;
+        p.work = m;
+        p.d.n = m;
+        p.d.nst = (int)rad.size();
+        for (int i = 0; i < p.d.nst; i++) p.d.radix[i] = rad[i];
+        fill_twiddles(tw, m);
+        chirp.resize(n);
+        std::vector<std::complex<double>> cd(n);
+        for (int k = 0; k < n; k++) {
+            const long long k2 = ((long long)k * k) % (2LL * n);
+            const double a = -M_PI * (double)k2 / n;
+            cd[k] = {std::cos(a), std::sin(a)};
+            chirp[k] = make_float2((float)cd[k].real(), (float)cd[k].imag());
+        }
+        std::vector<std::complex<double>> b(m, 0.0);
+        b[0] = std::conj(cd[0]);
+        for (int k = 1; k < n; k++) b[k] = b[m - k] = std::conj(cd[k]);
+        host_fft_pow2(b, -1);
+        bhat.resize(m);
+        for (int k = 0; k < m; k++) bhat[k] = make_float2((float)(b[k].real() / m), (float)(b[k].imag() / m));
+    }
+    const size_t cnt = tw.size() + chirp.size() + bhat.size();
+    h.bytes = cnt * sizeof(float2);
+    AT3R_CUDA(cudaMalloc(&h.d_tables, h.bytes));
+    std::vector<float2> all;
+    all.reserve(cnt);
+    all.insert(all.end(), tw.begin(), tw.end());
+    all.insert(all.end(), chirp.begin(), chirp.end());
+    all.insert(all.end(), bhat.begin(), bhat.end());
+    AT3R_CUDA(cudaMemcpy(h.d_tables, all.data(), h.bytes, cudaMemcpyHostToDevice));
+    p.d.tw = h.d_tables;
+    p.chirp = chirp.empty() ? nullptr : h.d_tables + tw.size();
+    p.bhat = bhat.empty() ? nullptr : h.d_tables + tw.size() + chirp.size();
+    return AT3R_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Which convention does the system cuFFT use for a 2-D C2R of (nz x nx)?
+// A pure-imaginary DC bin is invisible under the Hermitian reading and shows
+// up as -1/+1 on even/odd samples under half-length packing.  libcufft is
+// opened at run time, only for this question, once per size.
+// ---------------------------------------------------------------------------
+int probe_cufft_c2r(int nz, int nx)
+{
+    static std::mutex mu;
+    static std::map<std::pair<int, int>, int> cache;
+    std::lock_guard<std::mutex> lk(mu);
+    auto key = std::make_pair(nz, nx);
+    auto it = cache.find(key);
+    if (it != cache.end()) return it->second;
+    int result = AT3R_C2R_HERMITIAN;
+    static void* lib = nullptr;
+    if (!lib) {
+        for (const char* name : {"/usr/local/cuda/lib64/libcufft.so.11", "libcufft.so.11", "libcufft.so.12", "libcufft.so"}) {
+            lib = dlopen(name, RTLD_NOW | RTLD_LOCAL);
+            if (lib) break;
+        }
+    }
+    if (lib) {
+        typedef int (*plan2d_t)(int*, int, int, int);
+        typedef int (*exec_t)(int, void*, float*);
+        typedef int (*destroy_t)(int);
+        auto plan2d = (plan2d_t)dlsym(lib, "cufftPlan2d");
+        auto exec = (exec_t)dlsym(lib, "cufftExecC2R");
+        auto destroy = (destroy_t)dlsym(lib, "cufftDestroy");
+        if (plan2d && exec && destroy) {
+            const int kx = nx / 2 + 1;
+            const size_t elems = (size_t)nz * kx;
+            float2* d = nullptr;
+            if (cudaMalloc(&d, elems * sizeof(float2)) == cudaSuccess) {
+                cudaMemset(d, 0, elems * sizeof(float2));
+                const float2 one_i = make_float2(0.f, 1.f);
+                cudaMemcpy(d, &one_i, sizeof(float2), cudaMemcpyHostToDevice);
+                int plan = 0;
+                if (plan2d(&plan, nz, nx, 0x2c /* CUFFT_C2R */) == 0) {
+                    if (exec(plan, d, reinterpret_cast<float*>(d)) == 0) {
+                        float o[2] = {0.f, 0.f};
+                        cudaMemcpy(o, d, sizeof(o), cudaMemcpyDeviceToHost);
+                        if (std::fabs(o[0]) > 0.5f) result = AT3R_C2R_PACKED;
+                    }
+                    destroy(plan);
+                }
+                cudaFree(d);
+            }
+            cudaGetLastError();
+        }
+    }
+    cache[key] = result;
+    return result;
+}
+
+int round_up(int a, int b) { return (a + b - 1) / b * b; }
+
+}  // namespace
+
+struct at3r_plan {
+    at3r_geom g{};
+    std::vector<float> tilts;
+    int nx = 0, ny = 0, T = 0, N = 0, Nx = 0, Nz = 0, KX = 0;
+    int slab = 1;
+    int device = 0;
+    int c2r = AT3R_C2R_HERMITIAN;
+    float relax = 1.f;
+    std::vector<int> sub_start, sub_size;
+    float2* d_cs = nullptr;
+    // SART
+    float* d_raw = nullptr;
+    float* d_diff = nullptr;
+    int* d_flags = nullptr;
+    double* d_rf = nullptr;
+    std::vector<double> h_rf;
+    // WBP
+    float* d_h = nullptr;
+    float* d_filt = nullptr;
+    float* d_g2 = nullptr;    // also holds the cropped spectrum w
+    float2* d_y = nullptr;
+    HostFft fN, f2x, f2z, fz, fx;
+    int zcrop_cb = 4, zcrop_pitch = 0;
+    size_t smem_rweight = 0, smem_row = 0, smem_zcrop = 0, smem_xc2r = 0;
+    int bp_ww_sart = 0, bp_ww_wbp = 0;
+    // host path
+    float* d_proj_slab[2] = {nullptr, nullptr};
+    float* d_vol_slab[2] = {nullptr, nullptr};
+    cudaStream_t s_copy_in = nullptr, s_copy_out = nullptr;
+    cudaEvent_t ev[8] = {};
+    size_t ws_bytes = 0;
+    int64_t launches = 0;
+};
+
+namespace {
+
+template <typename T>
+at3r_status dalloc(at3r_plan* p, T** ptr, size_t count)
+{
+    const size_t bytes = count * sizeof(T);
+    cudaError_t e = cudaMalloc((void**)ptr, bytes);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return set_err(AT3R_ERR_OUT_OF_MEMORY, "cudaMalloc of " + std::to_string(bytes) + " bytes failed");
+    }
+    p->ws_bytes += bytes;
+    return AT3R_OK;
+}
+
+int bp_window(int tx, int tz, double scale, const std::vector<float>& cs, int T)
+{
+    double span = 0;
+    for (int t = 0; t < T; t++)
+        span = std::max(span, (std::fabs(cs[2 * t]) * (tx - 1) + std::fabs(cs[2 * t + 1]) * (tz - 1)) * scale);
+    return (int)std::ceil(span) + 6;
+}
+
+size_t bp_smem(int nt, int ww) { return sizeof(int) * ((nt + 3) & ~3) + sizeof(float) * (size_t)nt * ww; }
+
+// Every plan raises a kernel's dynamic shared-memory limit to the device
+// maximum (once per kernel and device), so plans of different sizes can
+// coexist; the amount a launch uses is still its own.
+at3r_status set_smem(const void* fn, size_t bytes)
+{
+    constexpr size_t kMax = 227 * 1024;
+    if (bytes > kMax)
+        return set_err(AT3R_ERR_TOO_LARGE, "shared-memory need " + std::to_string(bytes) + " exceeds 227 KB");
+    static std::mutex mu;
+    static std::map<std::pair<const void*, int>, bool> done;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    std::lock_guard<std::mutex> lk(mu);
+    if (!done[{fn, dev}]) {
+        AT3R_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMax));
+        done[{fn, dev}] = true;
+    }
+    return AT3R_OK;
+}
+
+#define CHECK_LAUNCH(p)                                                                   \
+    do {                                                                                  \
+        (p)->launches++;                                                                  \
+        cudaError_t e_ = cudaGetLastError();                                              \
+        if (e_ != cudaSuccess) return set_err(AT3R_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e_)); \
+    } while (0)
+
+// One slab of slices [y0, y0 + S): proj points at tilt 0 row 0 of a
+// [T][rows][nx] block whose row `proj_y0` is slice y0; vol points at the
+// slab's first output slice.
+at3r_status run_slab(at3r_plan* p, const float* proj, size_t tilt_stride, int proj_y0, int S, float* vol,
+                     cudaStream_t st)
+{
+    const int T = p->T, N = p->N, Nx = p->Nx, Nz = p->Nz;
+    if (p->g.method == AT3R_SART) {
+        k_gather_weight<<<dim3(T, S), 256, 0, st>>>(proj, tilt_stride, p->nx, proj_y0, p->d_cs, T, N, Nz, p->d_raw);
+        CHECK_LAUNCH(p);
+        AT3R_CUDA(cudaMemsetAsync(vol, 0, sizeof(float) * (size_t)S * Nx * Nz, st));
+        AT3R_CUDA(cudaMemsetAsync(p->d_flags, 0, sizeof(int) * S, st));
+        BpArgs a{};
+        a.T = T; a.N = N; a.cs = p->d_cs; a.GX = Nx; a.GZ = Nz;
+        a.out = vol; a.out_slice = (size_t)Nx * Nz; a.ww = p->bp_ww_sart; a.flags = p->d_flags;
+        const dim3 bgrid((Nx + BP_TX - 1) / BP_TX, (Nz + BP_TZ - 1) / BP_TZ, S);
+        // first back-projection: all tilts, relax 1 (CTomoSart.cpp:68-69)
+        a.sino = p->d_raw; a.t0 = 0; a.t1 = T; a.relax = 1.f;
+        k_bp<0><<<bgrid, BP_THREADS, bp_smem(T, a.ww), st>>>(a);
+        CHECK_LAUNCH(p);
+        a.sino = p->d_diff; a.relax = p->relax;
+        for (int it = 0; it < p->g.iterations; it++) {
+            for (size_t s = 0; s < p->sub_start.size(); s++) {
+                const int t0 = p->sub_start[s] + p->g.start_tilt, nt = p->sub_size[s];
+                if (nt <= 0) continue;
+                k_fp_diff<<<dim3((N + 255) / 256, nt, S), 256, 0, st>>>(
+                    vol, Nx, Nz, p->d_raw, p->d_diff, p->d_cs, T, N, t0,
+                    p->g.compute_rfactor ? p->d_rf + 2 * it : nullptr);
+                CHECK_LAUNCH(p);
+                a.t0 = t0; a.t1 = t0 + nt;
+                k_bp<0><<<bgrid, BP_THREADS, bp_smem(nt, a.ww), st>>>(a);
+                CHECK_LAUNCH(p);
+            }
+        }
+        k_fill_empty<<<S, 256, 0, st>>>(vol, (size_t)Nx * Nz, p->d_flags);
+        CHECK_LAUNCH(p);
+        return AT3R_OK;
+    }
+    // WBP
+    k_rweight<<<dim3((T + 1) / 2, S), 512, p->smem_rweight, st>>>(proj, tilt_stride, p->nx, proj_y0, p->d_cs, T, N,
+                                                                  Nz, p->d_h, p->fN.plan, p->d_filt);
+    CHECK_LAUNCH(p);
+    BpArgs a{};
+    a.sino = p->d_filt; a.T = T; a.N = N; a.t0 = 0; a.t1 = T; a.cs = p->d_cs;
+    a.GX = 2 * Nx; a.GZ = 2 * Nz; a.relax = 1.f; a.out = p->d_g2; a.out_slice = (size_t)4 * Nx * Nz;
+    a.ww = p->bp_ww_wbp; a.flags = nullptr;
+    const dim3 bgrid((2 * Nx + BP_TX - 1) / BP_TX, (2 * Nz + BP_TZ - 1) / BP_TZ, S);
+    k_bp<1><<<bgrid, BP_THREADS, bp_smem(T, a.ww), st>>>(a);
+    CHECK_LAUNCH(p);
+    k_row_r2c<<<dim3(Nz, S), 512, p->smem_row, st>>>(p->d_g2, Nx, Nz, p->f2x.plan, p->d_y);
+    CHECK_LAUNCH(p);
+    const float norm = (float)(1.0 / (2.0 * Nx) / (2.0 * Nz));
+    float2* w = reinterpret_cast<float2*>(p->d_g2);
+    k_zcrop<<<dim3((p->KX + p->zcrop_cb - 1) / p->zcrop_cb, S), 512, p->smem_zcrop, st>>>(
+        p->d_y, Nx, Nz, p->zcrop_cb, p->zcrop_pitch, p->f2z.plan, p->fz.plan, norm, w);
+    CHECK_LAUNCH(p);
+    k_x_c2r<<<dim3((Nz + 1) / 2, S), 512, p->smem_xc2r, st>>>(w, Nx, Nz, p->fx.plan, p->c2r == AT3R_C2R_PACKED, vol,
+                                                              (size_t)Nx * Nz);
+    CHECK_LAUNCH(p);
+    return AT3R_OK;
+}
+
+at3r_status begin_run(at3r_plan* p, cudaStream_t st)
+{
+    p->launches = 0;
+    int dev = -1;
+    AT3R_CUDA(cudaGetDevice(&dev));
+    if (dev != p->device) return set_err(AT3R_ERR_INVALID_ARGUMENT, "plan was created on another device");
+    if (p->g.method == AT3R_SART && p->g.compute_rfactor)
+        AT3R_CUDA(cudaMemsetAsync(p->d_rf, 0, sizeof(double) * 2 * std::max(1, p->g.iterations), st));
+    return AT3R_OK;
+}
+
+at3r_status end_run(at3r_plan* p, cudaStream_t st)
+{
+    if (p->g.method == AT3R_SART && p->g.compute_rfactor && p->g.iterations > 0)
+        AT3R_CUDA(cudaMemcpyAsync(p->h_rf.data(), p->d_rf, sizeof(double) * 2 * p->g.iterations,
+                                  cudaMemcpyDeviceToHost, st));
+    return AT3R_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+void at3r_geom_init(at3r_geom* g, int method)
+{
+    if (!g) return;
+    std::memset(g, 0, sizeof(*g));
+    g->method = method;
+    g->iterations = method == AT3R_SART ? 20 : 0;
+    g->subsets = 1;
+    g->relax = 0.f;
+    g->storage = AT3R_STORE_F32;
+    g->c2r = AT3R_C2R_MATCH_CUFFT;
+}
+
+at3r_status at3r_plan_create(const at3r_geom* g, at3r_plan** out)
+{
+    if (!g || !out) return set_err(AT3R_ERR_INVALID_ARGUMENT, "null argument");
+    *out = nullptr;
+    if (g->nx < 4 || g->ny < 1 || g->n_tilts < 1 || g->vol_z < 2 || !g->tilts_deg)
+        return set_err(AT3R_ERR_INVALID_ARGUMENT, "sizes must satisfy nx >= 4, ny >= 1, n_tilts >= 1, vol_z >= 2");
+    if (g->method != AT3R_WBP && g->method != AT3R_SART)
+        return set_err(AT3R_ERR_INVALID_ARGUMENT, "method must be AT3R_WBP or AT3R_SART");
+    if (g->storage != AT3R_STORE_F32)
+        return set_err(AT3R_ERR_UNSUPPORTED, "reduced-precision storage is not available in this build");
+    if (g->method == AT3R_SART) {
+        if (g->subsets < 1 || g->iterations < 0)
+            return set_err(AT3R_ERR_INVALID_ARGUMENT, "SART needs subsets >= 1 and iterations >= 0");
+        if (g->start_tilt < 0 || g->num_tilts < 0 || g->start_tilt + g->num_tilts > g->n_tilts)
+            return set_err(AT3R_ERR_INVALID_ARGUMENT, "SART tilt range outside the series");
+    }
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return set_err(AT3R_ERR_NO_DEVICE, "no CUDA device");
+    }
+    at3r_plan* p = new at3r_plan();
+    p->g = *g;
+    p->tilts.assign(g->tilts_deg, g->tilts_deg + g->n_tilts);
+    p->g.tilts_deg = p->tilts.data();
+    p->nx = g->nx; p->ny = g->ny; p->T = g->n_tilts;
+    p->N = g->nx & ~1; p->Nx = p->N; p->Nz = g->vol_z; p->KX = p->Nx / 2 + 1;
+    cudaGetDevice(&p->device);
+
+    // geometry table exactly as CTomoBase::Setup builds it (CTomoBase.cpp:56-65)
+    std::vector<float> cs(2 * p->T);
+    for (int t = 0; t < p->T; t++) {
+        const float a = 0.017453f * p->tilts[t];
+        cs[2 * t] = std::cos(a);
+        cs[2 * t + 1] = std::sin(a);
+        if (!(cs[2 * t] > 1e-3f)) {
+            delete p;
+            return set_err(AT3R_ERR_INVALID_ARGUMENT, "tilt angles must satisfy |tilt| < 89.9 degrees");
+        }
+    }
+    auto fail = [&](at3r_status s) { at3r_plan_destroy(p); return s; };
+    at3r_status rc;
+    if ((rc = dalloc(p, &p->d_cs, p->T))) return fail(rc);
+    if (cudaMemcpy(p->d_cs, cs.data(), sizeof(float) * 2 * p->T, cudaMemcpyHostToDevice) != cudaSuccess)
+        return fail(set_err(AT3R_ERR_CUDA, "geometry upload failed"));
+
+    const size_t T = p->T, N = p->N, Nx = p->Nx, Nz = p->Nz, KX = p->KX;
+    size_t per_slice;
+    if (g->method == AT3R_SART) {
+        p->relax = g->relax > 0.f ? g->relax : 1.0f / (float)g->subsets;
+        // AreTomo/Util/CSplitItems.cpp:25-48
+        const int n = g->num_tilts, k = g->subsets;
+        p->sub_size.assign(k, n / k);
+        p->sub_start.assign(k, 0);
+        for (int i = 0; i < n % k; i++) p->sub_size[i]++;
+        for (int i = 1; i < k; i++) p->sub_start[i] = p->sub_start[i - 1] + p->sub_size[i - 1];
+        p->bp_ww_sart = bp_window(BP_TX, BP_TZ, 1.0, cs, p->T);
+        if ((rc = set_smem((const void*)k_bp<0>, bp_smem(p->T, p->bp_ww_sart)))) return fail(rc);
+        per_slice = 2 * T * N * sizeof(float) + Nx * Nz * sizeof(float);
+    } else {
+        p->c2r = g->c2r == AT3R_C2R_MATCH_CUFFT ? probe_cufft_c2r(p->Nz, p->Nx) : g->c2r;
+        if ((rc = make_fft(p->N, p->fN))) return fail(rc);
+        if ((rc = make_fft(2 * p->Nx, p->f2x))) return fail(rc);
+        if ((rc = make_fft(2 * p->Nz, p->f2z))) return fail(rc);
+        if ((rc = make_fft(p->Nz, p->fz))) return fail(rc);
+        if ((rc = make_fft(p->Nx, p->fx))) return fail(rc);
+        p->smem_rweight = 2 * sizeof(float2) * p->fN.plan.work;
+        p->smem_row = 2 * sizeof(float2) * p->f2x.plan.work;
+        p->smem_xc2r = 2 * sizeof(float2) * p->fx.plan.work;
+        p->zcrop_pitch = round_up(std::max(p->f2z.plan.work, p->fz.plan.work), 2) + 1;
+        p->zcrop_cb = 4;
+        while (p->zcrop_cb > 1 && 2 * sizeof(float2) * p->zcrop_cb * p->zcrop_pitch > 227 * 1024) p->zcrop_cb /= 2;
+        p->smem_zcrop = 2 * sizeof(float2) * p->zcrop_cb * p->zcrop_pitch;
+        p->bp_ww_wbp = bp_window(BP_TX, BP_TZ, 0.5, cs, p->T);
+        if ((rc = set_smem((const void*)k_rweight, p->smem_rweight))) return fail(rc);
+        if ((rc = set_smem((const void*)k_row_r2c, p->smem_row))) return fail(rc);
+        if ((rc = set_smem((const void*)k_zcrop, p->smem_zcrop))) return fail(rc);
+        if ((rc = set_smem((const void*)k_x_c2r, p->smem_xc2r))) return fail(rc);
+        if ((rc = set_smem((const void*)k_bp<1>, bp_smem(p->T, p->bp_ww_wbp)))) return fail(rc);
+        // R-weight transfer function (GRWeight.cu:15-20), 1/N folded in
+        std::vector<float> h(N / 2 + 1);
+        const double twopi = (double)6.2831852f;
+        for (size_t k = 0; k <= N / 2; k++) {
+            const double f = (double)k / (double)N;
+            h[k] = (float)((1.0 / N) * 2.0 * f * (0.55 + 0.45 * std::cos(twopi * f)));
+        }
+        if ((rc = dalloc(p, &p->d_h, h.size()))) return fail(rc);
+        cudaMemcpy(p->d_h, h.data(), sizeof(float) * h.size(), cudaMemcpyHostToDevice);
+        per_slice = T * N * sizeof(float) + 16 * Nx * Nz + 2 * Nz * KX * sizeof(float2);
+    }
+
+    // slab: enough slices to fill the GPU, small enough to stay near L2
+    int slab = g->slab_slices;
+    if (slab <= 0) {
+        const size_t budget = g->method == AT3R_SART ? ((size_t)96 << 20) : ((size_t)256 << 20);
+        slab = (int)std::max<size_t>(1, budget / per_slice);
+        slab = std::max(slab, 8);
+    }
+    p->slab = std::min(slab, p->ny);
+    const size_t S = p->slab;
+    if (g->method == AT3R_SART) {
+        if ((rc = dalloc(p, &p->d_raw, S * T * N))) return fail(rc);
+        if ((rc = dalloc(p, &p->d_diff, S * T * N))) return fail(rc);
+        if ((rc = dalloc(p, &p->d_flags, S))) return fail(rc);
+        if ((rc = dalloc(p, &p->d_rf, 2 * (size_t)std::max(1, g->iterations)))) return fail(rc);
+        p->h_rf.assign(2 * std::max(1, g->iterations), 0.0);
+    } else {
+        if ((rc = dalloc(p, &p->d_filt, S * T * N))) return fail(rc);
+        if ((rc = dalloc(p, &p->d_g2, S * 4 * Nx * Nz))) return fail(rc);
+        if ((rc = dalloc(p, &p->d_y, S * 2 * Nz * KX))) return fail(rc);
+    }
+    *out = p;
+    return AT3R_OK;
+}
+
+void at3r_plan_destroy(at3r_plan* p)
+{
+    if (!p) return;
+    cudaFree(p->d_cs); cudaFree(p->d_raw); cudaFree(p->d_diff); cudaFree(p->d_flags); cudaFree(p->d_rf);
+    cudaFree(p->d_h); cudaFree(p->d_filt); cudaFree(p->d_g2); cudaFree(p->d_y);
+    for (HostFft* f : {&p->fN, &p->f2x, &p->f2z, &p->fz, &p->fx}) cudaFree(f->d_tables);
+    for (int i = 0; i < 2; i++) { cudaFree(p->d_proj_slab[i]); cudaFree(p->d_vol_slab[i]); }
+    if (p->s_copy_in) cudaStreamDestroy(p->s_copy_in);
+    if (p->s_copy_out) cudaStreamDestroy(p->s_copy_out);
+    for (cudaEvent_t& e : p->ev) if (e) cudaEventDestroy(e);
+    delete p;
+}
+
+at3r_status at3r_run_device(at3r_plan* p, const float* proj, float* vol, void* stream)
+{
+    if (!p || !proj || !vol) return set_err(AT3R_ERR_INVALID_ARGUMENT, "null argument");
+    cudaStream_t st = (cudaStream_t)stream;
+    at3r_status rc;
+    if ((rc = begin_run(p, st))) return rc;
+    const size_t tilt_stride = (size_t)p->ny * p->nx;
+    for (int y0 = 0; y0 < p->ny; y0 += p->slab) {
+        const int S = std::min(p->slab, p->ny - y0);
+        if ((rc = run_slab(p, proj, tilt_stride, y0, S, vol + (size_t)y0 * p->Nx * p->Nz, st))) return rc;
+    }
+    return end_run(p, st);
+}
+
+at3r_status at3r_run_host(at3r_plan* p, const float* const* frames, float* const* vol_frames, void* stream)
+{
+    if (!p || !frames || !vol_frames) return set_err(AT3R_ERR_INVALID_ARGUMENT, "null argument");
+    for (int t = 0; t < p->T; t++)
+        if (!frames[t]) return set_err(AT3R_ERR_INVALID_ARGUMENT, "null tilt frame");
+    for (int y = 0; y < p->ny; y++)
+        if (!vol_frames[y]) return set_err(AT3R_ERR_INVALID_ARGUMENT, "null volume frame");
+    cudaStream_t st = (cudaStream_t)stream;
+    const size_t S = p->slab, nx = p->nx, T = p->T, slice = (size_t)p->Nx * p->Nz;
+    at3r_status rc;
+    if (!p->d_proj_slab[0]) {
+        for (int i = 0; i < 2; i++) {
+            if ((rc = dalloc(p, &p->d_proj_slab[i], T * S * nx))) return rc;
+            if ((rc = dalloc(p, &p->d_vol_slab[i], S * slice))) return rc;
+        }
+        AT3R_CUDA(cudaStreamCreateWithFlags(&p->s_copy_in, cudaStreamNonBlocking));
+        AT3R_CUDA(cudaStreamCreateWithFlags(&p->s_copy_out, cudaStreamNonBlocking));
+        for (cudaEvent_t& e : p->ev) AT3R_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    }
+    if ((rc = begin_run(p, st))) return rc;
+    // ev[0,1]: input slab i copied; ev[2,3]: slab i computed; ev[4,5]: output slab i copied out
+    const int nslab = (p->ny + p->slab - 1) / p->slab;
+    auto copy_in = [&](int k) -> at3r_status {
+        const int b = k & 1, y0 = k * p->slab, n = std::min(p->slab, p->ny - y0);
+        if (k >= 2) AT3R_CUDA(cudaStreamWaitEvent(p->s_copy_in, p->ev[2 + b], 0));
+        for (int t = 0; t < p->T; t++)
+            AT3R_CUDA(cudaMemcpyAsync(p->d_proj_slab[b] + (size_t)t * S * nx, frames[t] + (size_t)y0 * nx,
+                                      sizeof(float) * n * nx, cudaMemcpyHostToDevice, p->s_copy_in));
+        AT3R_CUDA(cudaEventRecord(p->ev[b], p->s_copy_in));
+        return AT3R_OK;
+    };
+    if ((rc = copy_in(0))) return rc;
+    for (int k = 0; k < nslab; k++) {
+        const int b = k & 1, y0 = k * p->slab, n = std::min(p->slab, p->ny - y0);
+        if (k + 1 < nslab && (rc = copy_in(k + 1))) return rc;
+        AT3R_CUDA(cudaStreamWaitEvent(st, p->ev[b], 0));
+        if (k >= 2) AT3R_CUDA(cudaStreamWaitEvent(st, p->ev[4 + b], 0));
+        if ((rc = run_slab(p, p->d_proj_slab[b], S * nx, 0, n, p->d_vol_slab[b], st))) return rc;
+        AT3R_CUDA(cudaEventRecord(p->ev[2 + b], st));
+        AT3R_CUDA(cudaStreamWaitEvent(p->s_copy_out, p->ev[2 + b], 0));
+        for (int j = 0; j < n; j++)
+            AT3R_CUDA(cudaMemcpyAsync(vol_frames[y0 + j], p->d_vol_slab[b] + (size_t)j * slice, sizeof(float) * slice,
+                                      cudaMemcpyDeviceToHost, p->s_copy_out));
+        AT3R_CUDA(cudaEventRecord(p->ev[4 + b], p->s_copy_out));
+    }
+    AT3R_CUDA(cudaStreamWaitEvent(st, p->ev[4 + ((nslab - 1) & 1)], 0));
+    if ((rc = end_run(p, st))) return rc;
+    AT3R_CUDA(cudaStreamSynchronize(st));
+    return AT3R_OK;
+}
+
+at3r_status at3r_get_rfactor(const at3r_plan* p, double* out, int n)
+{
+    if (!p || !out) return set_err(AT3R_ERR_INVALID_ARGUMENT, "null argument");
+    if (p->g.method != AT3R_SART || !p->g.compute_rfactor)
+        return set_err(AT3R_ERR_INVALID_ARGUMENT, "plan does not compute the R-factor");
+    const int m = std::min(n, 2 * p->g.iterations);
+    for (int i = 0; i < m; i++) out[i] = p->h_rf[i];
+    return AT3R_OK;
+}
+
+size_t at3r_plan_workspace_bytes(const at3r_plan* p) { return p ? p->ws_bytes : 0; }
+int64_t at3r_plan_last_launches(const at3r_plan* p) { return p ? p->launches : 0; }
+int at3r_plan_c2r(const at3r_plan* p) { return p ? p->c2r : 0; }
+
+const char* at3r_status_str(at3r_status s)
+{
+    switch (s) {
+        case AT3R_OK: return "ok";
+        case AT3R_ERR_INVALID_ARGUMENT: return "invalid argument";
+        case AT3R_ERR_CUDA: return "CUDA error";
+        case AT3R_ERR_OUT_OF_MEMORY: return "out of device memory";
+        case AT3R_ERR_UNSUPPORTED: return "unsupported option";
+        case AT3R_ERR_TOO_LARGE: return "size exceeds a kernel limit";
+        case AT3R_ERR_NO_DEVICE: return "no CUDA device";
+    }
+    return "unknown status";
+}
+
+const char* at3r_last_error(void) { return g_last_error.c_str(); }
+
+}  // extern "C"

@@ -1,0 +1,230 @@
+"""Python binding of the at3r C ABI (include/at3r.h) and a mirror of the
+reference's reconstruction entry points.
+
+    vol = CDoWbpRecon().DoIt(tilt_series, align_param, vol_z)
+    vol = CDoSartRecon().DoIt(tilt_series, align_param, start_tilt, num_tilts, vol_z, iterations, subsets)
+
+follow ``MAR::CDoWbpRecon::DoIt`` / ``MAR::CDoSartRecon::DoIt``
+(AreTomo/Recon/CReconInc.h:259-306): the tilt series is read, not modified;
+the returned volume holds one XZ slice per y with z flipped, shape
+(ny, vol_z, nx & ~1).  Errors raise ``ReconError`` instead of aborting.
+
+All computation runs in libat3r.so on the GPU; there is no CPU path.
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from ._lib import load_library
+
+WBP, SART = 0, 1
+STORE_F32, STORE_F16, STORE_BF16 = 0, 1, 2
+C2R_MATCH_CUFFT, C2R_HERMITIAN, C2R_PACKED = 0, 1, 2
+
+
+class ReconError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"at3r status {status}: {message}")
+        self.status = status
+
+
+class Geom(ctypes.Structure):
+    _fields_ = [
+        ("nx", ctypes.c_int), ("ny", ctypes.c_int), ("n_tilts", ctypes.c_int),
+        ("tilts_deg", ctypes.POINTER(ctypes.c_float)),
+        ("vol_z", ctypes.c_int),
+        ("method", ctypes.c_int),
+        ("start_tilt", ctypes.c_int), ("num_tilts", ctypes.c_int),
+        ("iterations", ctypes.c_int), ("subsets", ctypes.c_int),
+        ("relax", ctypes.c_float),
+        ("storage", ctypes.c_int),
+        ("c2r", ctypes.c_int),
+        ("slab_slices", ctypes.c_int),
+        ("compute_rfactor", ctypes.c_int),
+    ]
+
+
+_EXPORTS = {
+    "at3r_geom_init": (None, [ctypes.POINTER(Geom), ctypes.c_int]),
+    "at3r_plan_create": (ctypes.c_int, [ctypes.POINTER(Geom), ctypes.POINTER(ctypes.c_void_p)]),
+    "at3r_plan_destroy": (None, [ctypes.c_void_p]),
+    "at3r_run_device": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
+    "at3r_run_host": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p),
+                                     ctypes.POINTER(ctypes.c_void_p), ctypes.c_void_p]),
+    "at3r_get_rfactor": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double), ctypes.c_int]),
+    "at3r_plan_workspace_bytes": (ctypes.c_size_t, [ctypes.c_void_p]),
+    "at3r_plan_last_launches": (ctypes.c_int64, [ctypes.c_void_p]),
+    "at3r_plan_c2r": (ctypes.c_int, [ctypes.c_void_p]),
+    "at3r_status_str": (ctypes.c_char_p, [ctypes.c_int]),
+    "at3r_last_error": (ctypes.c_char_p, []),
+}
+
+
+def lib() -> ctypes.CDLL:
+    L = load_library("libat3r.so")
+    if not getattr(L, "_at3r_typed", False):
+        for name, (res, args) in _EXPORTS.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        L._at3r_typed = True
+    return L
+
+
+def _check(rc: int) -> None:
+    if rc != 0:
+        L = lib()
+        raise ReconError(rc, f"{L.at3r_status_str(rc).decode()}: {L.at3r_last_error().decode()}")
+
+
+class Plan:
+    """One reconstruction plan (geometry, parameters and device workspace)."""
+
+    def __init__(self, nx, ny, tilts_deg, vol_z, method=WBP, start_tilt=0, num_tilts=None, iterations=0,
+                 subsets=1, relax=0.0, storage=STORE_F32, c2r=C2R_MATCH_CUFFT, slab_slices=0,
+                 compute_rfactor=False):
+        L = lib()
+        self._tilts = np.ascontiguousarray(np.asarray(tilts_deg, dtype=np.float32))
+        g = Geom()
+        L.at3r_geom_init(ctypes.byref(g), method)
+        g.nx, g.ny, g.n_tilts = int(nx), int(ny), int(self._tilts.size)
+        g.tilts_deg = self._tilts.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+        g.vol_z = int(vol_z)
+        g.start_tilt = int(start_tilt)
+        g.num_tilts = int(self._tilts.size if num_tilts is None else num_tilts)
+        g.iterations, g.subsets, g.relax = int(iterations), int(subsets), float(relax)
+        g.storage, g.c2r, g.slab_slices = int(storage), int(c2r), int(slab_slices)
+        g.compute_rfactor = int(bool(compute_rfactor))
+        self.geom = g
+        self.method = method
+        self.iterations = int(iterations)
+        self.nx, self.ny, self.vol_z = int(nx), int(ny), int(vol_z)
+        self.Nx = self.nx & ~1
+        h = ctypes.c_void_p()
+        _check(L.at3r_plan_create(ctypes.byref(g), ctypes.byref(h)))
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().at3r_plan_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def volume_shape(self):
+        return (self.ny, self.vol_z, self.Nx)
+
+    def run_device(self, proj_ptr: int, vol_ptr: int, stream: int = 0) -> None:
+        """proj_ptr / vol_ptr: device addresses of float[T][ny][nx] / float[ny][Nz][Nx]."""
+        _check(lib().at3r_run_device(self._h, ctypes.c_void_p(proj_ptr), ctypes.c_void_p(vol_ptr),
+                                     ctypes.c_void_p(stream)))
+
+    def run_host(self, frames, vol_frames, stream: int = 0) -> None:
+        """frames: sequence of T host float32 arrays [ny][nx]; vol_frames: ny host
+        float32 arrays [Nz][Nx], written in place."""
+        T = len(frames)
+        fin = (ctypes.c_void_p * T)(*[f.ctypes.data for f in frames])
+        fout = (ctypes.c_void_p * len(vol_frames))(*[v.ctypes.data for v in vol_frames])
+        _check(lib().at3r_run_host(self._h, fin, fout, ctypes.c_void_p(stream)))
+
+    def rfactor(self) -> np.ndarray:
+        """Per iteration (sum|raw - fp|, sum|raw|) of the last run."""
+        out = np.zeros(2 * max(self.iterations, 1), np.float64)
+        _check(lib().at3r_get_rfactor(self._h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), out.size))
+        return out[: 2 * self.iterations].reshape(self.iterations, 2)
+
+    @property
+    def workspace_bytes(self) -> int:
+        return int(lib().at3r_plan_workspace_bytes(self._h))
+
+    @property
+    def last_launches(self) -> int:
+        return int(lib().at3r_plan_last_launches(self._h))
+
+    @property
+    def c2r(self) -> int:
+        return int(lib().at3r_plan_c2r(self._h))
+
+
+# --- reference-shaped entry points -----------------------------------------
+
+@dataclass
+class TiltSeries:
+    """The aligned tilt series: frames[T][ny][nx] float32 (MD::CTiltSeries)."""
+    frames: np.ndarray
+
+    @property
+    def stk_size(self):
+        t, ny, nx = self.frames.shape
+        return (nx, ny, t)
+
+
+@dataclass
+class AlignParam:
+    """Per-tilt angles in degrees, alpha offset folded in (MAM::CAlignParam::GetTilts)."""
+    tilts: np.ndarray = field(default_factory=lambda: np.zeros(0, np.float32))
+
+    def GetTilts(self, copy: bool = False):
+        return self.tilts.copy() if copy else self.tilts
+
+
+def _host_run(plan: Plan, frames: np.ndarray) -> np.ndarray:
+    frames = np.ascontiguousarray(frames, dtype=np.float32)
+    vol = np.empty(plan.volume_shape, np.float32)
+    plan.run_host([frames[t] for t in range(frames.shape[0])], [vol[y] for y in range(vol.shape[0])])
+    return vol
+
+
+class CDoWbpRecon:
+    """MAR::CDoWbpRecon (AreTomo/Recon/CDoWbpRecon.cpp:28-47)."""
+
+    def __init__(self, **options):
+        self.options = options
+
+    def DoIt(self, tilt_series: TiltSeries, align_param: AlignParam, vol_z: int) -> np.ndarray:
+        nx, ny, nt = tilt_series.stk_size
+        plan = Plan(nx, ny, align_param.GetTilts(False)[:nt], vol_z, method=WBP, **self.options)
+        try:
+            return _host_run(plan, tilt_series.frames)
+        finally:
+            plan.close()
+
+
+class CDoSartRecon:
+    """MAR::CDoSartRecon (AreTomo/Recon/CDoSartRecon.cpp:30-57)."""
+
+    def __init__(self, **options):
+        self.options = options
+
+    def DoIt(self, tilt_series: TiltSeries, align_param: AlignParam, start_tilt: int, num_tilts: int, vol_z: int,
+             iterations: int, subsets: int) -> np.ndarray:
+        nx, ny, nt = tilt_series.stk_size
+        plan = Plan(nx, ny, align_param.GetTilts(False)[:nt], vol_z, method=SART, start_tilt=start_tilt,
+                    num_tilts=num_tilts, iterations=iterations, subsets=subsets, **self.options)
+        try:
+            return _host_run(plan, tilt_series.frames)
+        finally:
+            plan.close()
+
+
+def reconstruct_device(proj, tilts, vol_z, method=WBP, out=None, stream=None, **kw):
+    """Device-resident reconstruction of a torch CUDA tensor proj[T][ny][nx]
+    (float32, contiguous).  Returns (or fills) vol[ny][vol_z][nx & ~1]."""
+    import torch
+    if not (proj.is_cuda and proj.dtype == torch.float32 and proj.is_contiguous()):
+        raise ValueError("proj must be a contiguous float32 CUDA tensor")
+    T, ny, nx = proj.shape
+    plan = Plan(nx, ny, tilts, vol_z, method=method, **kw)
+    if out is None:
+        out = torch.empty(plan.volume_shape, device=proj.device, dtype=torch.float32)
+    s = stream if stream is not None else torch.cuda.current_stream(proj.device)
+    plan.run_device(proj.data_ptr(), out.data_ptr(), s.cuda_stream)
+    return out, plan

@@ -1,0 +1,116 @@
+/*
+ * at3r — B200-native tomographic reconstruction (WBP and SART) with the
+ * semantics of AreTomo3's AreTomo/Recon, behind a C ABI.
+ *
+ * Geometry: single-axis parallel beam, tilt axis along y, tilt angles in
+ * degrees (alpha offset already folded in, as CAlignParam::GetTilts(false)
+ * returns them).  Every y-slice (XZ plane) is reconstructed from row y of
+ * every tilt image.
+ *
+ * Sizes (as in the reference):
+ *   nx, ny, n_tilts   projection width, height and count
+ *   Nx = nx & ~1      volume width (an odd last column is ignored)
+ *   Nz = vol_z        volume thickness
+ * Data layouts:
+ *   projections, device : float proj[n_tilts][ny][nx]  (x fastest)
+ *   projections, host   : n_tilts frame pointers, each float[ny][nx]
+ *   volume, device      : float vol[ny][Nz][Nx]  — frame y is the XZ slice at
+ *                         y with z flipped, exactly the frames that
+ *                         CDoWbpRecon::DoIt / CDoSartRecon::DoIt return
+ *   volume, host        : ny frame pointers, each float[Nz][Nx]
+ *
+ * Errors are returned as status codes; nothing aborts the process.  A plan is
+ * not safe to run from two host threads at once; distinct plans are
+ * independent (no module-global device state).  `stream` is a cudaStream_t
+ * (NULL = the legacy default stream).
+ */
+#ifndef AT3R_H
+#define AT3R_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum at3r_status {
+    AT3R_OK = 0,
+    AT3R_ERR_INVALID_ARGUMENT = 1,
+    AT3R_ERR_CUDA = 2,
+    AT3R_ERR_OUT_OF_MEMORY = 3,
+    AT3R_ERR_UNSUPPORTED = 4,
+    AT3R_ERR_TOO_LARGE = 5,
+    AT3R_ERR_NO_DEVICE = 6
+} at3r_status;
+
+typedef enum at3r_method { AT3R_WBP = 0, AT3R_SART = 1 } at3r_method;
+
+/* Storage type of the staged projections (WBP: the filtered sinogram; SART:
+ * the weighted sinogram and the residual).  Accumulation is FP32 always. */
+typedef enum at3r_storage { AT3R_STORE_F32 = 0, AT3R_STORE_F16 = 1, AT3R_STORE_BF16 = 2 } at3r_storage;
+
+/* How the final complex-to-real inverse FFT of the WBP Fourier crop treats
+ * the imaginary parts of its DC and Nyquist bins (the cropped spectrum is
+ * not Hermitian there).  cuFFT, which the reference calls, picks per size:
+ * most sizes drop them (HERMITIAN); some (e.g. 1200 x 4096) use a
+ * half-length packing algorithm that folds them into even/odd samples
+ * (PACKED).  MATCH_CUFFT asks the system cuFFT once per size which it does,
+ * so the output equals the reference's; it falls back to HERMITIAN when
+ * libcufft cannot be loaded. */
+typedef enum at3r_c2r { AT3R_C2R_MATCH_CUFFT = 0, AT3R_C2R_HERMITIAN = 1, AT3R_C2R_PACKED = 2 } at3r_c2r;
+
+typedef struct at3r_geom {
+    int nx, ny, n_tilts;
+    const float* tilts_deg;   /* [n_tilts]; copied by at3r_plan_create */
+    int vol_z;                /* Nz */
+    int method;               /* at3r_method */
+    /* SART only (CDoSartRecon::DoIt arguments): subsets partition tilts
+     * [start_tilt, start_tilt + num_tilts); the first back-projection uses
+     * all n_tilts. */
+    int start_tilt, num_tilts;
+    int iterations, subsets;
+    float relax;              /* <= 0: 1/subsets, the reference's rule */
+    int storage;              /* at3r_storage */
+    int c2r;                  /* at3r_c2r (WBP only) */
+    int slab_slices;          /* y-slices per device batch; 0 = automatic */
+    int compute_rfactor;      /* SART: accumulate per-iteration residual sums */
+} at3r_geom;
+
+typedef struct at3r_plan at3r_plan;
+
+/* Fills g with the reference's defaults for the method (relax = 1/subsets,
+ * FP32 storage, cuFFT-matching C2R, automatic slabs). */
+void at3r_geom_init(at3r_geom* g, int method);
+
+/* Validates g, uploads the geometry table and allocates the device workspace
+ * on the current device. */
+at3r_status at3r_plan_create(const at3r_geom* g, at3r_plan** out);
+void at3r_plan_destroy(at3r_plan* plan);
+
+/* Device-resident form: proj and vol are device pointers in the layouts above. */
+at3r_status at3r_run_device(at3r_plan* plan, const float* proj, float* vol, void* stream);
+
+/* Host form (the reference's CDoWbpRecon/CDoSartRecon data flow): reads the
+ * tilt frames from host memory, writes the volume frames to host memory,
+ * overlapping copies with compute; returns after the volume is on the host. */
+at3r_status at3r_run_host(at3r_plan* plan, const float* const* frames, float* const* vol_frames, void* stream);
+
+/* SART residual sums of the last run: per iteration, sum|raw - fp| and
+ * sum|raw| over valid detector samples (FP64).  out holds 2 * iterations. */
+at3r_status at3r_get_rfactor(const at3r_plan* plan, double* out, int n);
+
+/* Bytes of device workspace the plan holds. */
+size_t at3r_plan_workspace_bytes(const at3r_plan* plan);
+/* Number of kernel launches issued by the last run. */
+int64_t at3r_plan_last_launches(const at3r_plan* plan);
+/* Which C2R convention the plan resolved to (AT3R_C2R_HERMITIAN/PACKED). */
+int at3r_plan_c2r(const at3r_plan* plan);
+
+const char* at3r_status_str(at3r_status s);
+const char* at3r_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,64 @@
+"""CPU checks of the C ABI: the library loads, exports every function that
+include/at3r.h declares, and rejects invalid geometry before touching a GPU."""
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+from oracle_lib import ROOT
+
+
+def declared_functions():
+    src = open(os.path.join(ROOT, "include", "at3r.h")).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"\b(at3r_[a-z0-9_]+)\s*\(", src)))
+
+
+def test_header_declares_the_entry_points():
+    names = declared_functions()
+    for n in ("at3r_plan_create", "at3r_plan_destroy", "at3r_run_device", "at3r_run_host", "at3r_status_str"):
+        assert n in names
+
+
+def test_library_exports_every_declared_function():
+    from aretomo3_b200 import recon
+    L = recon.lib()
+    missing = [n for n in declared_functions() if not hasattr(L, n)]
+    assert not missing, missing
+
+
+def test_status_strings():
+    from aretomo3_b200 import recon
+    L = recon.lib()
+    for s in range(7):
+        assert L.at3r_status_str(s)
+    assert L.at3r_status_str(0) == b"ok"
+
+
+@pytest.mark.parametrize("kw", [
+    dict(nx=2),                                   # too narrow
+    dict(vol_z=1),                                # too thin
+    dict(method=7),                               # unknown method
+    dict(method=1, subsets=0, iterations=1),      # SART without subsets
+    dict(method=1, start_tilt=8, num_tilts=8),    # tilt range outside the series
+])
+def test_invalid_geometry_is_rejected_without_gpu(kw):
+    from aretomo3_b200 import recon
+    args = dict(nx=64, ny=4, vol_z=16, method=0, subsets=1)
+    args.update(kw)
+    tilts = np.linspace(-60, 60, 11).astype(np.float32)
+    with pytest.raises(recon.ReconError) as ei:
+        recon.Plan(args.pop("nx"), args.pop("ny"), tilts, args.pop("vol_z"), **args)
+    assert ei.value.status == 1  # AT3R_ERR_INVALID_ARGUMENT
+
+
+def test_valid_geometry_without_gpu_reports_no_device():
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    from aretomo3_b200 import recon
+    with pytest.raises(recon.ReconError) as ei:
+        recon.Plan(64, 4, np.linspace(-60, 60, 11), 16)
+    assert ei.value.status == 6  # AT3R_ERR_NO_DEVICE

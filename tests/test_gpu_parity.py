@@ -1,0 +1,204 @@
+"""GPU parity: the CUDA path (through the C ABI) against the reference's own
+CUDA Recon — the committed golden fixtures, and live runs of the reference
+binary (oracle/_ref/ref_recon) on larger inputs — and against the FP64
+oracle.
+
+Tolerances (relative L2 over the volume):
+  * vs the reference's CUDA output: 1e-4 (plain FP32 bar).  Sample selection
+    and tilt order match the reference, so agreement is ~1e-6 in practice.
+  * vs the FP64 oracle: 1e-4.
+"""
+import os
+import sys
+
+import numpy as np
+import pytest
+
+from oracle_lib import ROOT, load_golden, rel_l2, sart, wbp
+
+pytestmark = pytest.mark.gpu
+
+REF_TOL = 1e-4
+ORACLE_TOL = 1e-4
+REF_BIN = os.path.join(ROOT, "oracle", "_ref", "ref_recon")
+
+
+@pytest.fixture(scope="module")
+def R():
+    import torch
+    assert torch.cuda.is_available(), "GPU tests need a CUDA device"
+    from aretomo3_b200 import recon
+    return recon
+
+
+def run_reference(*a, **k):
+    if not os.path.exists(REF_BIN):
+        pytest.skip("reference binary oracle/_ref/ref_recon not built")
+    sys.path.insert(0, os.path.join(ROOT, "tests", "golden"))
+    import gen_golden
+    return gen_golden.run_reference(*a, **k)[0]
+
+
+def ours(R, frames, tilts, meta, **opts):
+    ts = R.TiltSeries(np.ascontiguousarray(frames))
+    ap = R.AlignParam(np.asarray(tilts, np.float32))
+    if meta["mode"] == "wbp":
+        return R.CDoWbpRecon(**opts).DoIt(ts, ap, meta["vol_z"])
+    return R.CDoSartRecon(**opts).DoIt(ts, ap, meta["start"], meta["ntilts"], meta["vol_z"], meta["iters"],
+                                       meta["subsets"])
+
+
+GOLDEN = ["wbp_128", "wbp_odd97", "wbp_160", "wbp_512_rows", "sart_128", "sart_odd97", "sart_1k_row"]
+
+
+@pytest.mark.parametrize("name", GOLDEN)
+def test_matches_reference_golden(R, name):
+    frames, tilts, ref, meta = load_golden(name)
+    out = ours(R, frames, tilts, meta)
+    assert out.shape == ref.shape
+    err = rel_l2(out, ref)
+    print(f"{name}: rel-L2 vs reference {err:.3e}, max-abs {np.abs(out - ref).max():.3e}")
+    assert err < REF_TOL
+
+
+@pytest.mark.parametrize("name", ["wbp_128", "sart_128"])
+def test_device_path_equals_host_path(R, name):
+    import torch
+    frames, tilts, _, meta = load_golden(name)
+    host = ours(R, frames, tilts, meta)
+    proj = torch.from_numpy(np.ascontiguousarray(frames)).cuda()
+    kw = dict(method=R.WBP) if meta["mode"] == "wbp" else dict(
+        method=R.SART, start_tilt=meta["start"], num_tilts=meta["ntilts"], iterations=meta["iters"],
+        subsets=meta["subsets"])
+    vol, plan = R.reconstruct_device(proj, tilts, meta["vol_z"], **kw)
+    torch.cuda.synchronize()
+    assert np.array_equal(vol.cpu().numpy(), host)
+
+
+@pytest.mark.parametrize("slab", [1, 3])
+def test_slab_size_does_not_change_result(R, slab):
+    frames, tilts, _, meta = load_golden("sart_128")
+    a = ours(R, frames, tilts, meta)
+    b = ours(R, frames, tilts, meta, slab_slices=slab)
+    assert np.array_equal(a, b)
+    frames, tilts, _, meta = load_golden("wbp_odd97")
+    a = ours(R, frames, tilts, meta)
+    b = ours(R, frames, tilts, meta, slab_slices=slab)
+    assert np.array_equal(a, b)
+
+
+def _series(nx, ny, tilts, vol_z, seed, noise=1):
+    from aretomo3_b200 import synth
+    ph = synth.Phantom(seed=seed, n_ellipsoids=60, axis_min=3, axis_max=20, n_beads=6, bead_radius=3,
+                       noise_kind=noise, noise_param=0.1 if noise == 1 else 50.0)
+    return synth.make_tilt_series(nx, ny, tilts, vol_z, ph)
+
+
+def test_wbp_512_full_series_vs_reference(R):
+    """The 512x512x41 WBP series (thickness 128) end to end against the
+    reference binary run live on the same input."""
+    from aretomo3_b200 import synth
+    c = synth.wbp_small()
+    frames = synth.make_tilt_series(c["nx"], c["ny"], c["tilts"], c["vol_z"], c["phantom"])
+    ref = run_reference("wbp", frames, c["tilts"], c["vol_z"])
+    out = ours(R, frames, c["tilts"], dict(mode="wbp", vol_z=c["vol_z"]))
+    err = rel_l2(out, ref)
+    print(f"WBP 512x512x41 rel-L2 vs reference {err:.3e}")
+    assert err < REF_TOL
+
+
+def test_sart_1k_slab_vs_reference(R):
+    """16 rows of the 1024x1024x61 SART series (thickness 300, 15 iterations,
+    5 subsets) against the reference binary."""
+    from aretomo3_b200 import synth
+    c = synth.sart_1k()
+    frames = synth.make_tilt_series(c["nx"], c["ny"], c["tilts"], c["vol_z"], c["phantom"])
+    frames = np.ascontiguousarray(frames[:, 500:516, :])
+    ref = run_reference("sart", frames, c["tilts"], c["vol_z"], 0, 61, 15, 5)
+    meta = dict(mode="sart", vol_z=300, start=0, ntilts=61, iters=15, subsets=5)
+    out = ours(R, frames, c["tilts"], meta)
+    err = rel_l2(out, ref)
+    print(f"SART 1k slab rel-L2 vs reference {err:.3e}")
+    assert err < REF_TOL
+
+
+def test_wbp_4k_rows_vs_reference_packed_c2r(R):
+    """Two rows of a 4096-wide series at thickness 1200: the size at which the
+    reference's cuFFT C2R uses half-length packing.  The plan must detect it
+    and match."""
+    from aretomo3_b200 import synth
+    tilts = synth.tilt_range(-60, 60, 3)
+    frames = _series(4096, 2, tilts, 1200, seed=41)
+    ref = run_reference("wbp", frames, tilts, 1200)
+    plan = R.Plan(4096, 2, tilts, 1200, method=R.WBP)
+    assert plan.c2r == R.C2R_PACKED
+    plan.close()
+    out = ours(R, frames, tilts, dict(mode="wbp", vol_z=1200))
+    err = rel_l2(out, ref)
+    print(f"WBP 4096 x 1200 rows rel-L2 vs reference {err:.3e}")
+    assert err < REF_TOL
+    # and the FP64 oracle under the same convention
+    o64 = wbp(frames, tilts, 1200, c2r_mode=1)
+    assert rel_l2(out, o64) < ORACLE_TOL
+
+
+@pytest.mark.parametrize("nx,vol_z,ntilt", [(1198, 300, 41), (768, 599, 31), (130, 64, 5), (512, 97, 61)])
+def test_wbp_odd_and_bluestein_sizes_vs_oracle(R, nx, vol_z, ntilt):
+    """FFT lengths with large prime factors (2*599, 599, 2*65=130 -> 13*5*2)
+    take the Bluestein or generic-radix paths."""
+    tilts = np.linspace(-58, 61, ntilt).astype(np.float32)
+    frames = _series(nx, 2, tilts, vol_z, seed=nx + vol_z)
+    out = ours(R, frames, tilts, dict(mode="wbp", vol_z=vol_z))
+    plan = R.Plan(nx, 2, tilts, vol_z, method=R.WBP)
+    mode = 1 if plan.c2r == R.C2R_PACKED else 0
+    plan.close()
+    o64 = wbp(frames, tilts, vol_z, c2r_mode=mode)
+    err = rel_l2(out, o64)
+    print(f"WBP nx={nx} Nz={vol_z} T={ntilt}: rel-L2 vs FP64 oracle {err:.3e}")
+    assert err < ORACLE_TOL
+
+
+@pytest.mark.parametrize("start,num,iters,subsets", [(0, 31, 0, 1), (2, 25, 2, 30), (5, 20, 3, 7), (0, 31, 1, 31)])
+def test_sart_edge_parameters_vs_oracle(R, start, num, iters, subsets):
+    """No iterations; more subsets than tilts (empty subsets do nothing); a
+    sub-range of tilts; one tilt per subset."""
+    tilts = np.linspace(-60, 60, 31).astype(np.float32)
+    frames = _series(96, 3, tilts, 40, seed=7, noise=2)
+    meta = dict(mode="sart", vol_z=40, start=start, ntilts=num, iters=iters, subsets=subsets)
+    out = ours(R, frames, tilts, meta)
+    o64 = sart(frames, tilts, 40, start, num, iters, subsets)
+    assert rel_l2(out, o64) < ORACLE_TOL
+
+
+def test_sart_rfactor_decreases_and_matches_oracle(R):
+    from aretomo3_b200 import synth
+    tilts = synth.tilt_range(-60, 60, 4)
+    frames = _series(128, 4, tilts, 40, seed=3, noise=0)
+    plan = R.Plan(128, 4, tilts, 40, method=R.SART, iterations=6, subsets=5, compute_rfactor=True)
+    vol = np.empty(plan.volume_shape, np.float32)
+    plan.run_host([frames[t] for t in range(tilts.size)], [vol[y] for y in range(4)])
+    rf = plan.rfactor()
+    plan.close()
+    r = rf[:, 0] / rf[:, 1]
+    assert np.all(np.diff(r) < 0), r
+    _, rf64 = sart(frames, tilts, 40, 0, tilts.size, 6, 5, rfactor=True)
+    assert np.allclose(rf, rf64, rtol=1e-4)
+
+
+def test_single_slice_single_tilt(R):
+    tilts = np.array([7.5], np.float32)
+    frames = _series(64, 1, tilts, 16, seed=5)
+    for meta in (dict(mode="wbp", vol_z=16), dict(mode="sart", vol_z=16, start=0, ntilts=1, iters=2, subsets=1)):
+        out = ours(R, frames, tilts, meta)
+        ref = wbp(frames, tilts, 16) if meta["mode"] == "wbp" else sart(frames, tilts, 16, 0, 1, 2, 1)
+        assert rel_l2(out, ref) < ORACLE_TOL
+
+
+def test_invalid_arguments_raise(R):
+    tilts = np.linspace(-60, 60, 11).astype(np.float32)
+    with pytest.raises(R.ReconError):
+        R.Plan(64, 4, tilts, 16, method=R.SART, start_tilt=5, num_tilts=10, iterations=1, subsets=2)
+    with pytest.raises(R.ReconError):
+        R.Plan(64, 4, np.array([90.0], np.float32), 16)
+    with pytest.raises(R.ReconError):
+        R.Plan(64, 4, tilts, 16, method=R.SART, iterations=1, subsets=0)
