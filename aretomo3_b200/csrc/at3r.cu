@@ -200,6 +200,15 @@ int probe_cufft_c2r(int nz, int nx)
 
 int round_up(int a, int b) { return (a + b - 1) / b * b; }
 
+enum KernelKind { KK_GATHER, KK_RWEIGHT, KK_BP_SART, KK_BP_WBP, KK_FP_DIFF, KK_FILL, KK_ROW_R2C, KK_ZCROP, KK_XC2R,
+                  KK_COUNT };
+const char* kKernelNames[KK_COUNT] = {"gather_weight", "rweight", "bp_sart", "bp_wbp_2x", "fp_diff",
+                                      "fill_empty", "row_r2c", "zcrop", "x_c2r"};
+struct KStat {
+    int64_t launches;
+    double bytes, units, ms;
+};
+
 }  // namespace
 
 struct at3r_plan {
@@ -234,6 +243,13 @@ struct at3r_plan {
     cudaEvent_t ev[8] = {};
     size_t ws_bytes = 0;
     int64_t launches = 0;
+    // per-kernel accounting of the last run; device times only with timing on
+    bool timing = false;
+    std::vector<cudaEvent_t> evpool;
+    size_t evused = 0;
+    std::vector<std::pair<int, size_t>> pending;  // (kind, index of the start event)
+    KStat stats[KK_COUNT] = {};
+    std::vector<int> ray_len;                     // forward-projection samples per ray, per tilt
 };
 
 namespace {
@@ -281,11 +297,50 @@ at3r_status set_smem(const void* fn, size_t bytes)
     return AT3R_OK;
 }
 
-#define CHECK_LAUNCH(p)                                                                   \
-    do {                                                                                  \
-        (p)->launches++;                                                                  \
-        cudaError_t e_ = cudaGetLastError();                                              \
-        if (e_ != cudaSuccess) return set_err(AT3R_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e_)); \
+// Launch bookkeeping: tbegin/tend bracket every kernel launch.  With timing
+// enabled each launch is bracketed by two events on its own stream; the
+// algorithmic bytes (compulsory DRAM reads + writes) and work units of every
+// launch are tallied always.
+at3r_status tbegin(at3r_plan* p, cudaStream_t st)
+{
+    if (!p->timing) return AT3R_OK;
+    if (p->evused + 2 > p->evpool.size()) {
+        for (int i = 0; i < 256; i++) {
+            cudaEvent_t e;
+            AT3R_CUDA(cudaEventCreate(&e));
+            p->evpool.push_back(e);
+        }
+    }
+    AT3R_CUDA(cudaEventRecord(p->evpool[p->evused], st));
+    return AT3R_OK;
+}
+
+at3r_status tend(at3r_plan* p, cudaStream_t st, int kind, double bytes, double units)
+{
+    p->launches++;
+    KStat& k = p->stats[kind];
+    k.launches++;
+    k.bytes += bytes;
+    k.units += units;
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return set_err(AT3R_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e));
+    if (p->timing) {
+        AT3R_CUDA(cudaEventRecord(p->evpool[p->evused + 1], st));
+        p->pending.push_back({kind, p->evused});
+        p->evused += 2;
+    }
+    return AT3R_OK;
+}
+
+#define TB(p, st)                                  \
+    do {                                           \
+        at3r_status r_ = tbegin((p), (st));        \
+        if (r_ != AT3R_OK) return r_;              \
+    } while (0)
+#define TE(p, st, kind, bytes, units)                                  \
+    do {                                                               \
+        at3r_status r_ = tend((p), (st), (kind), (double)(bytes), (double)(units)); \
+        if (r_ != AT3R_OK) return r_;                                  \
     } while (0)
 
 // One slab of slices [y0, y0 + S): proj points at tilt 0 row 0 of a
@@ -294,10 +349,12 @@ at3r_status set_smem(const void* fn, size_t bytes)
 at3r_status run_slab(at3r_plan* p, const float* proj, size_t tilt_stride, int proj_y0, int S, float* vol,
                      cudaStream_t st)
 {
-    const int T = p->T, N = p->N, Nx = p->Nx, Nz = p->Nz;
+    const int T = p->T, N = p->N, Nx = p->Nx, Nz = p->Nz, KX = p->KX;
+    const double f4 = 4.0, vox = (double)S * Nx * Nz;
     if (p->g.method == AT3R_SART) {
+        TB(p, st);
         k_gather_weight<<<dim3(T, S), 256, 0, st>>>(proj, tilt_stride, p->nx, proj_y0, p->d_cs, T, N, Nz, p->d_raw);
-        CHECK_LAUNCH(p);
+        TE(p, st, KK_GATHER, 2 * f4 * S * T * N, (double)S * T * N);
         AT3R_CUDA(cudaMemsetAsync(vol, 0, sizeof(float) * (size_t)S * Nx * Nz, st));
         AT3R_CUDA(cudaMemsetAsync(p->d_flags, 0, sizeof(int) * S, st));
         BpArgs a{};
@@ -306,53 +363,67 @@ at3r_status run_slab(at3r_plan* p, const float* proj, size_t tilt_stride, int pr
         const dim3 bgrid((Nx + BP_TX - 1) / BP_TX, (Nz + BP_TZ - 1) / BP_TZ, S);
         // first back-projection: all tilts, relax 1 (CTomoSart.cpp:68-69)
         a.sino = p->d_raw; a.t0 = 0; a.t1 = T; a.relax = 1.f;
+        TB(p, st);
         k_bp<0><<<bgrid, BP_THREADS, bp_smem(T, a.ww), st>>>(a);
-        CHECK_LAUNCH(p);
+        TE(p, st, KK_BP_SART, f4 * (S * (double)T * N + 2 * vox), vox * T);
         a.sino = p->d_diff; a.relax = p->relax;
         for (int it = 0; it < p->g.iterations; it++) {
             for (size_t s = 0; s < p->sub_start.size(); s++) {
                 const int t0 = p->sub_start[s] + p->g.start_tilt, nt = p->sub_size[s];
                 if (nt <= 0) continue;
+                double samples = 0;
+                for (int t = t0; t < t0 + nt; t++) samples += (double)p->ray_len[t];
+                TB(p, st);
                 k_fp_diff<<<dim3((N + 255) / 256, nt, S), 256, 0, st>>>(
                     vol, Nx, Nz, p->d_raw, p->d_diff, p->d_cs, T, N, t0,
                     p->g.compute_rfactor ? p->d_rf + 2 * it : nullptr);
-                CHECK_LAUNCH(p);
+                TE(p, st, KK_FP_DIFF, f4 * (vox + 2.0 * S * nt * N), samples * N * S);
                 a.t0 = t0; a.t1 = t0 + nt;
+                TB(p, st);
                 k_bp<0><<<bgrid, BP_THREADS, bp_smem(nt, a.ww), st>>>(a);
-                CHECK_LAUNCH(p);
+                TE(p, st, KK_BP_SART, f4 * (S * (double)nt * N + 2 * vox), vox * nt);
             }
         }
+        TB(p, st);
         k_fill_empty<<<S, 256, 0, st>>>(vol, (size_t)Nx * Nz, p->d_flags);
-        CHECK_LAUNCH(p);
+        TE(p, st, KK_FILL, f4 * S, 0);
         return AT3R_OK;
     }
     // WBP
+    TB(p, st);
     k_rweight<<<dim3((T + 1) / 2, S), 512, p->smem_rweight, st>>>(proj, tilt_stride, p->nx, proj_y0, p->d_cs, T, N,
                                                                   Nz, p->d_h, p->fN.plan, p->d_filt);
-    CHECK_LAUNCH(p);
+    TE(p, st, KK_RWEIGHT, 2 * f4 * S * T * N, (double)S * T * N);
     BpArgs a{};
     a.sino = p->d_filt; a.T = T; a.N = N; a.t0 = 0; a.t1 = T; a.cs = p->d_cs;
     a.GX = 2 * Nx; a.GZ = 2 * Nz; a.relax = 1.f; a.out = p->d_g2; a.out_slice = (size_t)4 * Nx * Nz;
     a.ww = p->bp_ww_wbp; a.flags = nullptr;
     const dim3 bgrid((2 * Nx + BP_TX - 1) / BP_TX, (2 * Nz + BP_TZ - 1) / BP_TZ, S);
+    TB(p, st);
     k_bp<1><<<bgrid, BP_THREADS, bp_smem(T, a.ww), st>>>(a);
-    CHECK_LAUNCH(p);
+    TE(p, st, KK_BP_WBP, f4 * (S * (double)T * N + 4 * vox), 4 * vox * T);
+    TB(p, st);
     k_row_r2c<<<dim3(Nz, S), 512, p->smem_row, st>>>(p->d_g2, Nx, Nz, p->f2x.plan, p->d_y);
-    CHECK_LAUNCH(p);
+    TE(p, st, KK_ROW_R2C, f4 * 4 * vox + 8.0 * S * 2 * Nz * KX, 4 * vox);
     const float norm = (float)(1.0 / (2.0 * Nx) / (2.0 * Nz));
     float2* w = reinterpret_cast<float2*>(p->d_g2);
-    k_zcrop<<<dim3((p->KX + p->zcrop_cb - 1) / p->zcrop_cb, S), 512, p->smem_zcrop, st>>>(
+    TB(p, st);
+    k_zcrop<<<dim3((KX + p->zcrop_cb - 1) / p->zcrop_cb, S), 512, p->smem_zcrop, st>>>(
         p->d_y, Nx, Nz, p->zcrop_cb, p->zcrop_pitch, p->f2z.plan, p->fz.plan, norm, w);
-    CHECK_LAUNCH(p);
+    TE(p, st, KK_ZCROP, 8.0 * S * 3 * Nz * KX, (double)S * 2 * Nz * KX);
+    TB(p, st);
     k_x_c2r<<<dim3((Nz + 1) / 2, S), 512, p->smem_xc2r, st>>>(w, Nx, Nz, p->fx.plan, p->c2r == AT3R_C2R_PACKED, vol,
                                                               (size_t)Nx * Nz);
-    CHECK_LAUNCH(p);
+    TE(p, st, KK_XC2R, 8.0 * S * Nz * KX + f4 * vox, vox);
     return AT3R_OK;
 }
 
 at3r_status begin_run(at3r_plan* p, cudaStream_t st)
 {
     p->launches = 0;
+    p->evused = 0;
+    p->pending.clear();
+    for (KStat& k : p->stats) k = KStat{};
     int dev = -1;
     AT3R_CUDA(cudaGetDevice(&dev));
     if (dev != p->device) return set_err(AT3R_ERR_INVALID_ARGUMENT, "plan was created on another device");
@@ -425,6 +496,8 @@ at3r_status at3r_plan_create(const at3r_geom* g, at3r_plan** out)
             return set_err(AT3R_ERR_INVALID_ARGUMENT, "tilt angles must satisfy |tilt| < 89.9 degrees");
         }
     }
+    p->ray_len.resize(p->T);
+    for (int t = 0; t < p->T; t++) p->ray_len[t] = (int)((float)p->Nz / cs[2 * t] + 1.5f);
     auto fail = [&](at3r_status s) { at3r_plan_destroy(p); return s; };
     at3r_status rc;
     if ((rc = dalloc(p, &p->d_cs, p->T))) return fail(rc);
@@ -510,6 +583,7 @@ void at3r_plan_destroy(at3r_plan* p)
     if (p->s_copy_in) cudaStreamDestroy(p->s_copy_in);
     if (p->s_copy_out) cudaStreamDestroy(p->s_copy_out);
     for (cudaEvent_t& e : p->ev) if (e) cudaEventDestroy(e);
+    for (cudaEvent_t e : p->evpool) cudaEventDestroy(e);
     delete p;
 }
 
@@ -589,6 +663,38 @@ at3r_status at3r_get_rfactor(const at3r_plan* p, double* out, int n)
 }
 
 size_t at3r_plan_workspace_bytes(const at3r_plan* p) { return p ? p->ws_bytes : 0; }
+
+at3r_status at3r_plan_set_timing(at3r_plan* p, int enable)
+{
+    if (!p) return set_err(AT3R_ERR_INVALID_ARGUMENT, "null plan");
+    p->timing = enable != 0;
+    return AT3R_OK;
+}
+
+int at3r_plan_kernel_stats(at3r_plan* p, int kind, const char** name, int64_t* launches, double* ms, double* bytes,
+                           double* units)
+{
+    if (!p) return 0;
+    if (kind < 0 || kind >= KK_COUNT) return KK_COUNT;
+    if (p->timing && !p->pending.empty()) {
+        // resolve event pairs once the last one has completed
+        cudaEventSynchronize(p->evpool[p->pending.back().second + 1]);
+        for (KStat& k : p->stats) k.ms = 0;
+        for (auto& pr : p->pending) {
+            float t = 0.f;
+            if (cudaEventElapsedTime(&t, p->evpool[pr.second], p->evpool[pr.second + 1]) == cudaSuccess)
+                p->stats[pr.first].ms += t;
+        }
+        cudaGetLastError();
+    }
+    const KStat& k = p->stats[kind];
+    if (name) *name = kKernelNames[kind];
+    if (launches) *launches = k.launches;
+    if (ms) *ms = k.ms;
+    if (bytes) *bytes = k.bytes;
+    if (units) *units = k.units;
+    return KK_COUNT;
+}
 int64_t at3r_plan_last_launches(const at3r_plan* p) { return p ? p->launches : 0; }
 int at3r_plan_c2r(const at3r_plan* p) { return p ? p->c2r : 0; }
 

@@ -58,6 +58,10 @@ _EXPORTS = {
     "at3r_plan_workspace_bytes": (ctypes.c_size_t, [ctypes.c_void_p]),
     "at3r_plan_last_launches": (ctypes.c_int64, [ctypes.c_void_p]),
     "at3r_plan_c2r": (ctypes.c_int, [ctypes.c_void_p]),
+    "at3r_plan_set_timing": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "at3r_plan_kernel_stats": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_char_p),
+                                              ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_double),
+                                              ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]),
     "at3r_status_str": (ctypes.c_char_p, [ctypes.c_int]),
     "at3r_last_error": (ctypes.c_char_p, []),
 }
@@ -152,6 +156,25 @@ class Plan:
     @property
     def c2r(self) -> int:
         return int(lib().at3r_plan_c2r(self._h))
+
+    def set_timing(self, enable: bool) -> None:
+        _check(lib().at3r_plan_set_timing(self._h, int(bool(enable))))
+
+    def kernel_stats(self) -> dict:
+        """Per kernel kind of the last run: launches, device ms (timing on),
+        algorithmic bytes, work units."""
+        L = lib()
+        out = {}
+        n = L.at3r_plan_kernel_stats(self._h, 0, None, None, None, None, None)
+        for k in range(n):
+            name = ctypes.c_char_p()
+            la = ctypes.c_int64()
+            ms, by, un = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+            L.at3r_plan_kernel_stats(self._h, k, ctypes.byref(name), ctypes.byref(la), ctypes.byref(ms),
+                                     ctypes.byref(by), ctypes.byref(un))
+            if la.value:
+                out[name.value.decode()] = dict(launches=la.value, ms=ms.value, bytes=by.value, units=un.value)
+        return out
 
 
 # --- reference-shaped entry points -----------------------------------------

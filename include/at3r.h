@@ -102,6 +102,16 @@ at3r_status at3r_get_rfactor(const at3r_plan* plan, double* out, int n);
 
 /* Bytes of device workspace the plan holds. */
 size_t at3r_plan_workspace_bytes(const at3r_plan* plan);
+/* Per-kernel accounting.  With timing enabled, every kernel launch of a run
+ * is bracketed by CUDA events on its stream.  at3r_plan_kernel_stats reports,
+ * for kernel kind `kind` of the last run: its name, launches, device
+ * milliseconds (0 unless timing was on), algorithmic DRAM bytes (compulsory
+ * reads + writes of the data it consumes and produces) and work units
+ * (voxel x tilt updates; ray samples for the forward projection).  It
+ * returns the number of kinds and waits for the last run's events. */
+at3r_status at3r_plan_set_timing(at3r_plan* plan, int enable);
+int at3r_plan_kernel_stats(at3r_plan* plan, int kind, const char** name, int64_t* launches, double* ms,
+                           double* bytes, double* units);
 /* Number of kernel launches issued by the last run. */
 int64_t at3r_plan_last_launches(const at3r_plan* plan);
 /* Which C2R convention the plan resolved to (AT3R_C2R_HERMITIAN/PACKED). */
