@@ -54,6 +54,11 @@ def workload(name: str, seed_offset: int = 0) -> dict:
         c = synth.sart_1k(seed=2 + seed_offset)
         c.update(method="sart", relax=0.3, label="SART 1024x1024x61 tilts, thickness 300, 15 iterations, 5 subsets, "
                                                  "relaxation 0.3, Poisson 50 e-/px")
+    elif name == "sart_1k_small":
+        # profiling case: the same shape per slice, 128 rows (volume 157 MB > L2)
+        c = synth.sart_1k(seed=2 + seed_offset)
+        c.update(ny=128, method="sart", relax=0.3,
+                 label="SART 1024x128x61 tilts, thickness 300, 15 iterations, 5 subsets, relaxation 0.3")
     elif name == "sart_1k_ref_relax":
         c = synth.sart_1k(seed=2 + seed_offset)
         c.update(method="sart", relax=0.0, label="SART 1024x1024x61 tilts, thickness 300, 15 iterations, 5 subsets, "
