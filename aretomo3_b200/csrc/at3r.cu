@@ -715,3 +715,140 @@ const char* at3r_status_str(at3r_status s)
 const char* at3r_last_error(void) { return g_last_error.c_str(); }
 
 }  // extern "C"
+
+// ===========================================================================
+// SART without device allocation.
+//
+// Some callers cannot allocate device memory at the moment they reconstruct:
+// a host application whose allocator has already reserved the device's
+// memory (a cudaMalloc would fail or fragment its pool), or a pipeline that
+// keeps several series in flight on other streams (cudaMalloc and cudaFree
+// may synchronise the whole device and stall that work).  For them this
+// entry point runs the plain-FP32 SART path with its scratch — the per-tilt
+// cos/sin table, the weighted sinogram rows, the residual rows and the
+// per-slice sentinel flags — in one fixed array that lives in this library's
+// device image.  The caller passes the projections and the volume.
+//
+// The array is AT3R_NOALLOC_SCRATCH_BYTES (16 MiB) on every GPU the library
+// is loaded on, held until the process exits.  Every call shares it and it
+// keeps the last call's contents, so calls that overlap on the GPU (two
+// streams, two threads) race; serialise them.  The first call on a device
+// looks up the array's device address (and raises the back-projection
+// kernel's shared-memory limit); make that first call before any stream
+// capture.
+// ===========================================================================
+namespace {
+
+constexpr size_t kNoallocBytes = (size_t)16 << 20;
+constexpr int kNoallocMaxTilts = 4096;   // cos/sin table capacity
+constexpr int kNoallocMaxSlab = 8192;    // sentinel-flag capacity
+constexpr size_t kNoallocHeader = sizeof(float2) * kNoallocMaxTilts + sizeof(int) * kNoallocMaxSlab;
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoallocBytes];
+
+at3r_status noalloc_scratch_address(unsigned char** out)
+{
+    static std::mutex mu;
+    static std::map<int, unsigned char*> addr;
+    int dev = 0;
+    AT3R_CUDA(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> lk(mu);
+    auto it = addr.find(dev);
+    if (it != addr.end()) { *out = it->second; return AT3R_OK; }
+    void* ptr = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+    if (e != cudaSuccess || !ptr) {
+        cudaGetLastError();
+        return set_err(AT3R_ERR_CUDA, std::string("cudaGetSymbolAddress(no-allocation scratch): ") +
+                                          cudaGetErrorString(e));
+    }
+    at3r_status rc = set_smem((const void*)k_bp<0>, 0);
+    if (rc != AT3R_OK) return rc;
+    addr[dev] = (unsigned char*)ptr;
+    *out = (unsigned char*)ptr;
+    return AT3R_OK;
+}
+
+}  // namespace
+
+extern "C" at3r_status at3r_sart_device_noalloc(const float* proj, int nx, int ny, int n_tilts,
+                                                const float* tilts_deg, int vol_z, int start_tilt, int num_tilts,
+                                                int iterations, int subsets, float relax, float* vol, void* stream)
+{
+    if (!proj || !vol || !tilts_deg) return set_err(AT3R_ERR_INVALID_ARGUMENT, "null argument");
+    if (nx < 4 || ny < 1 || n_tilts < 1 || vol_z < 2)
+        return set_err(AT3R_ERR_INVALID_ARGUMENT, "sizes must satisfy nx >= 4, ny >= 1, n_tilts >= 1, vol_z >= 2");
+    if (subsets < 1 || iterations < 0)
+        return set_err(AT3R_ERR_INVALID_ARGUMENT, "SART needs subsets >= 1 and iterations >= 0");
+    if (start_tilt < 0 || num_tilts < 0 || start_tilt + num_tilts > n_tilts)
+        return set_err(AT3R_ERR_INVALID_ARGUMENT, "SART tilt range outside the series");
+    const int T = n_tilts, N = nx & ~1, Nx = N, Nz = vol_z;
+    if (T > kNoallocMaxTilts)
+        return set_err(AT3R_ERR_TOO_LARGE, "the no-allocation entry point takes at most " +
+                                               std::to_string(kNoallocMaxTilts) + " tilts");
+    const size_t per_slice = 2 * sizeof(float) * (size_t)T * N;
+    const size_t room = kNoallocBytes - kNoallocHeader;
+    if (per_slice > room)
+        return set_err(AT3R_ERR_TOO_LARGE,
+                       "the no-allocation scratch (16 MiB) holds the weighted sinogram and residual of at least one "
+                       "y-slice, 2 * n_tilts * (nx & ~1) floats; this series needs " +
+                           std::to_string(per_slice) + " bytes per slice, at most " + std::to_string(room));
+    std::vector<float> cs(2 * T);
+    for (int t = 0; t < T; t++) {
+        const float a = 0.017453f * tilts_deg[t];
+        cs[2 * t] = std::cos(a);
+        cs[2 * t + 1] = std::sin(a);
+        if (!(cs[2 * t] > 1e-3f))
+            return set_err(AT3R_ERR_INVALID_ARGUMENT, "tilt angles must satisfy |tilt| < 89.9 degrees");
+    }
+    const int ww = bp_window(BP_TX, BP_TZ, 1.0, cs, T);
+    if (bp_smem(T, ww) > 227 * 1024) return set_err(AT3R_ERR_TOO_LARGE, "back-projection window exceeds 227 KB");
+    unsigned char* base = nullptr;
+    at3r_status rc = noalloc_scratch_address(&base);
+    if (rc != AT3R_OK) return rc;
+    float2* d_cs = reinterpret_cast<float2*>(base);
+    int* d_flags = reinterpret_cast<int*>(base + sizeof(float2) * kNoallocMaxTilts);
+    const int slab = (int)std::min<size_t>({room / per_slice, (size_t)kNoallocMaxSlab, (size_t)ny});
+    float* d_raw = reinterpret_cast<float*>(base + kNoallocHeader);
+    float* d_diff = d_raw + (size_t)slab * T * N;
+    cudaStream_t st = (cudaStream_t)stream;
+    AT3R_CUDA(cudaMemcpyAsync(d_cs, cs.data(), sizeof(float) * 2 * T, cudaMemcpyHostToDevice, st));
+
+    // contiguous subsets of [start_tilt, start_tilt + num_tilts), the first n % k one larger
+    std::vector<int> sub_start(subsets, 0), sub_size(subsets, num_tilts / subsets);
+    for (int i = 0; i < num_tilts % subsets; i++) sub_size[i]++;
+    for (int i = 1; i < subsets; i++) sub_start[i] = sub_start[i - 1] + sub_size[i - 1];
+    const float rlx = relax > 0.f ? relax : 1.0f / (float)subsets;
+    const size_t tilt_stride = (size_t)ny * nx;
+    for (int y0 = 0; y0 < ny; y0 += slab) {
+        const int S = std::min(slab, ny - y0);
+        float* v = vol + (size_t)y0 * Nx * Nz;
+        k_gather_weight<<<dim3(T, S), 256, 0, st>>>(proj, tilt_stride, nx, y0, d_cs, T, N, Nz, d_raw);
+        AT3R_CUDA(cudaGetLastError());
+        AT3R_CUDA(cudaMemsetAsync(v, 0, sizeof(float) * (size_t)S * Nx * Nz, st));
+        AT3R_CUDA(cudaMemsetAsync(d_flags, 0, sizeof(int) * S, st));
+        BpArgs a{};
+        a.T = T; a.N = N; a.cs = d_cs; a.GX = Nx; a.GZ = Nz;
+        a.out = v; a.out_slice = (size_t)Nx * Nz; a.ww = ww; a.flags = d_flags;
+        const dim3 bgrid((Nx + BP_TX - 1) / BP_TX, (Nz + BP_TZ - 1) / BP_TZ, S);
+        a.sino = d_raw; a.t0 = 0; a.t1 = T; a.relax = 1.f;
+        k_bp<0><<<bgrid, BP_THREADS, bp_smem(T, ww), st>>>(a);
+        AT3R_CUDA(cudaGetLastError());
+        a.sino = d_diff; a.relax = rlx;
+        for (int it = 0; it < iterations; it++) {
+            for (int s = 0; s < subsets; s++) {
+                const int t0 = sub_start[s] + start_tilt, nt = sub_size[s];
+                if (nt <= 0) continue;
+                k_fp_diff<<<dim3((N + 255) / 256, nt, S), 256, 0, st>>>(v, Nx, Nz, d_raw, d_diff, d_cs, T, N, t0,
+                                                                        nullptr);
+                AT3R_CUDA(cudaGetLastError());
+                a.t0 = t0; a.t1 = t0 + nt;
+                k_bp<0><<<bgrid, BP_THREADS, bp_smem(nt, ww), st>>>(a);
+                AT3R_CUDA(cudaGetLastError());
+            }
+        }
+        k_fill_empty<<<S, 256, 0, st>>>(v, (size_t)Nx * Nz, d_flags);
+        AT3R_CUDA(cudaGetLastError());
+    }
+    return AT3R_OK;
+}

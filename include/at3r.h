@@ -117,6 +117,25 @@ int64_t at3r_plan_last_launches(const at3r_plan* plan);
 /* Which C2R convention the plan resolved to (AT3R_C2R_HERMITIAN/PACKED). */
 int at3r_plan_c2r(const at3r_plan* plan);
 
+/* SART of a device-resident series without allocating device memory.  No
+ * counterpart in the reference: it is for callers that cannot allocate when
+ * they reconstruct — an application whose own allocator already reserved the
+ * device's memory, or a pipeline with other series in flight that a
+ * cudaMalloc/cudaFree (which may synchronise the device) would stall.
+ * Arguments as in at3r_geom / CDoSartRecon::DoIt; relax <= 0 selects
+ * 1/subsets; FP32 storage; proj and vol are device pointers in the layouts
+ * above.  Scratch is one 16 MiB array in the library's device image on every
+ * GPU that loads the library, held until exit; it must hold
+ * 2 * n_tilts * (nx & ~1) floats for at least one y-slice (and n_tilts <=
+ * 4096), otherwise AT3R_ERR_TOO_LARGE.  Calls share that array and it keeps
+ * the last call's contents: calls that overlap on the GPU race, so serialise
+ * them.  The first call on a device does a one-time set-up (the array's
+ * device address, a kernel attribute); make it before any stream capture.
+ * Enqueues on `stream` and returns without waiting. */
+at3r_status at3r_sart_device_noalloc(const float* proj, int nx, int ny, int n_tilts, const float* tilts_deg,
+                                     int vol_z, int start_tilt, int num_tilts, int iterations, int subsets,
+                                     float relax, float* vol, void* stream);
+
 const char* at3r_status_str(at3r_status s);
 const char* at3r_last_error(void);
 
