@@ -275,7 +275,8 @@ int bp_window(int tx, int tz, double scale, const std::vector<float>& cs, int T)
     return (int)std::ceil(span) + 6;
 }
 
-size_t bp_smem(int nt, int ww) { return sizeof(int) * ((nt + 3) & ~3) + sizeof(float) * (size_t)nt * ww; }
+// tilts are staged in chunks, so the window buffer does not grow with the tilt count
+size_t bp_smem(int, int ww) { return bp_smem_bytes(ww); }
 
 // Every plan raises a kernel's dynamic shared-memory limit to the device
 // maximum (once per kernel and device), so plans of different sizes can
@@ -351,32 +352,34 @@ at3r_status run_slab(at3r_plan* p, const float* proj, size_t tilt_stride, int pr
 {
     const int T = p->T, N = p->N, Nx = p->Nx, Nz = p->Nz, KX = p->KX;
     const double f4 = 4.0, vox = (double)S * Nx * Nz;
+    const int SG = (S + SB - 1) / SB;   // slice groups: each thread carries SB slices
+    AT3R_CUDA(cudaMemsetAsync(p->d_flags, 0, sizeof(int) * S, st));
     if (p->g.method == AT3R_SART) {
         TB(p, st);
-        k_gather_weight<<<dim3(T, S), 256, 0, st>>>(proj, tilt_stride, p->nx, proj_y0, p->d_cs, T, N, Nz, p->d_raw);
+        k_gather_weight<<<dim3(T, S), 256, 0, st>>>(proj, tilt_stride, p->nx, proj_y0, p->d_cs, T, N, Nz, p->d_raw,
+                                                    p->d_flags);
         TE(p, st, KK_GATHER, 2 * f4 * S * T * N, (double)S * T * N);
         AT3R_CUDA(cudaMemsetAsync(vol, 0, sizeof(float) * (size_t)S * Nx * Nz, st));
-        AT3R_CUDA(cudaMemsetAsync(p->d_flags, 0, sizeof(int) * S, st));
         BpArgs a{};
-        a.T = T; a.N = N; a.cs = p->d_cs; a.GX = Nx; a.GZ = Nz;
+        a.T = T; a.N = N; a.cs = p->d_cs; a.GX = Nx; a.GZ = Nz; a.S = S;
         a.out = vol; a.out_slice = (size_t)Nx * Nz; a.ww = p->bp_ww_sart; a.flags = p->d_flags;
-        const dim3 bgrid((Nx + BP_TX - 1) / BP_TX, (Nz + BP_TZ - 1) / BP_TZ, S);
+        const dim3 bgrid((Nx + BP_TX - 1) / BP_TX, (Nz + BP_TZ - 1) / BP_TZ, SG);
         // first back-projection: all tilts, relax 1 (CTomoSart.cpp:68-69)
-        a.sino = p->d_raw; a.t0 = 0; a.t1 = T; a.relax = 1.f;
+        a.sino = p->d_raw; a.t0 = 0; a.t1 = T; a.relax = 1.f; a.low_bit = kFlagRawLow;
         TB(p, st);
         k_bp<0><<<bgrid, BP_THREADS, bp_smem(T, a.ww), st>>>(a);
         TE(p, st, KK_BP_SART, f4 * (S * (double)T * N + 2 * vox), vox * T);
-        a.sino = p->d_diff; a.relax = p->relax;
+        a.sino = p->d_diff; a.relax = p->relax; a.low_bit = kFlagDiffLow;
         for (int it = 0; it < p->g.iterations; it++) {
             for (size_t s = 0; s < p->sub_start.size(); s++) {
                 const int t0 = p->sub_start[s] + p->g.start_tilt, nt = p->sub_size[s];
                 if (nt <= 0) continue;
                 double samples = 0;
                 for (int t = t0; t < t0 + nt; t++) samples += (double)p->ray_len[t];
+                double* rfp = p->g.compute_rfactor ? p->d_rf + 2 * it : nullptr;
                 TB(p, st);
-                k_fp_diff<<<dim3((N + 255) / 256, nt, S), 256, 0, st>>>(
-                    vol, Nx, Nz, p->d_raw, p->d_diff, p->d_cs, T, N, t0,
-                    p->g.compute_rfactor ? p->d_rf + 2 * it : nullptr);
+                k_fp_diff<<<dim3((N + 255) / 256, nt, SG), 256, 0, st>>>(vol, Nx, Nz, S, p->d_raw, p->d_diff,
+                                                                         p->d_cs, T, N, t0, rfp, p->d_flags);
                 TE(p, st, KK_FP_DIFF, f4 * (vox + 2.0 * S * nt * N), samples * N * S);
                 a.t0 = t0; a.t1 = t0 + nt;
                 TB(p, st);
@@ -392,13 +395,13 @@ at3r_status run_slab(at3r_plan* p, const float* proj, size_t tilt_stride, int pr
     // WBP
     TB(p, st);
     k_rweight<<<dim3((T + 1) / 2, S), 512, p->smem_rweight, st>>>(proj, tilt_stride, p->nx, proj_y0, p->d_cs, T, N,
-                                                                  Nz, p->d_h, p->fN.plan, p->d_filt);
+                                                                  Nz, p->d_h, p->fN.plan, p->d_filt, p->d_flags);
     TE(p, st, KK_RWEIGHT, 2 * f4 * S * T * N, (double)S * T * N);
     BpArgs a{};
     a.sino = p->d_filt; a.T = T; a.N = N; a.t0 = 0; a.t1 = T; a.cs = p->d_cs;
-    a.GX = 2 * Nx; a.GZ = 2 * Nz; a.relax = 1.f; a.out = p->d_g2; a.out_slice = (size_t)4 * Nx * Nz;
-    a.ww = p->bp_ww_wbp; a.flags = nullptr;
-    const dim3 bgrid((2 * Nx + BP_TX - 1) / BP_TX, (2 * Nz + BP_TZ - 1) / BP_TZ, S);
+    a.GX = 2 * Nx; a.GZ = 2 * Nz; a.S = S; a.relax = 1.f; a.out = p->d_g2; a.out_slice = (size_t)4 * Nx * Nz;
+    a.ww = p->bp_ww_wbp; a.flags = p->d_flags; a.low_bit = kFlagRawLow;
+    const dim3 bgrid((2 * Nx + BP_TX - 1) / BP_TX, (2 * Nz + BP_TZ - 1) / BP_TZ, SG);
     TB(p, st);
     k_bp<1><<<bgrid, BP_THREADS, bp_smem(T, a.ww), st>>>(a);
     TE(p, st, KK_BP_WBP, f4 * (S * (double)T * N + 4 * vox), 4 * vox * T);
@@ -566,6 +569,7 @@ at3r_status at3r_plan_create(const at3r_geom* g, at3r_plan** out)
         p->h_rf.assign(2 * std::max(1, g->iterations), 0.0);
     } else {
         if ((rc = dalloc(p, &p->d_filt, S * T * N))) return fail(rc);
+        if ((rc = dalloc(p, &p->d_flags, S))) return fail(rc);
         if ((rc = dalloc(p, &p->d_g2, S * 4 * Nx * Nz))) return fail(rc);
         if ((rc = dalloc(p, &p->d_y, S * 2 * Nz * KX))) return fail(rc);
     }
@@ -696,6 +700,8 @@ int at3r_plan_kernel_stats(at3r_plan* p, int kind, const char** name, int64_t* l
     return KK_COUNT;
 }
 int64_t at3r_plan_last_launches(const at3r_plan* p) { return p ? p->launches : 0; }
+
+
 int at3r_plan_c2r(const at3r_plan* p) { return p ? p->c2r : 0; }
 
 const char* at3r_status_str(at3r_status s)
@@ -823,24 +829,25 @@ extern "C" at3r_status at3r_sart_device_noalloc(const float* proj, int nx, int n
     for (int y0 = 0; y0 < ny; y0 += slab) {
         const int S = std::min(slab, ny - y0);
         float* v = vol + (size_t)y0 * Nx * Nz;
-        k_gather_weight<<<dim3(T, S), 256, 0, st>>>(proj, tilt_stride, nx, y0, d_cs, T, N, Nz, d_raw);
+        const int SG = (S + SB - 1) / SB;
+        AT3R_CUDA(cudaMemsetAsync(d_flags, 0, sizeof(int) * S, st));
+        k_gather_weight<<<dim3(T, S), 256, 0, st>>>(proj, tilt_stride, nx, y0, d_cs, T, N, Nz, d_raw, d_flags);
         AT3R_CUDA(cudaGetLastError());
         AT3R_CUDA(cudaMemsetAsync(v, 0, sizeof(float) * (size_t)S * Nx * Nz, st));
-        AT3R_CUDA(cudaMemsetAsync(d_flags, 0, sizeof(int) * S, st));
         BpArgs a{};
-        a.T = T; a.N = N; a.cs = d_cs; a.GX = Nx; a.GZ = Nz;
+        a.T = T; a.N = N; a.cs = d_cs; a.GX = Nx; a.GZ = Nz; a.S = S;
         a.out = v; a.out_slice = (size_t)Nx * Nz; a.ww = ww; a.flags = d_flags;
-        const dim3 bgrid((Nx + BP_TX - 1) / BP_TX, (Nz + BP_TZ - 1) / BP_TZ, S);
-        a.sino = d_raw; a.t0 = 0; a.t1 = T; a.relax = 1.f;
+        const dim3 bgrid((Nx + BP_TX - 1) / BP_TX, (Nz + BP_TZ - 1) / BP_TZ, SG);
+        a.sino = d_raw; a.t0 = 0; a.t1 = T; a.relax = 1.f; a.low_bit = kFlagRawLow;
         k_bp<0><<<bgrid, BP_THREADS, bp_smem(T, ww), st>>>(a);
         AT3R_CUDA(cudaGetLastError());
-        a.sino = d_diff; a.relax = rlx;
+        a.sino = d_diff; a.relax = rlx; a.low_bit = kFlagDiffLow;
         for (int it = 0; it < iterations; it++) {
             for (int s = 0; s < subsets; s++) {
                 const int t0 = sub_start[s] + start_tilt, nt = sub_size[s];
                 if (nt <= 0) continue;
-                k_fp_diff<<<dim3((N + 255) / 256, nt, S), 256, 0, st>>>(v, Nx, Nz, d_raw, d_diff, d_cs, T, N, t0,
-                                                                        nullptr);
+                k_fp_diff<<<dim3((N + 255) / 256, nt, SG), 256, 0, st>>>(v, Nx, Nz, S, d_raw, d_diff, d_cs, T, N,
+                                                                         t0, nullptr, d_flags);
                 AT3R_CUDA(cudaGetLastError());
                 a.t0 = t0; a.t1 = t0 + nt;
                 k_bp<0><<<bgrid, BP_THREADS, bp_smem(nt, ww), st>>>(a);

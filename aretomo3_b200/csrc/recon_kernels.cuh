@@ -12,6 +12,7 @@
 #include <cuda_fp16.h>
 #include <cuda_bf16.h>
 #include <stdint.h>
+#include <climits>
 
 #include "fft_smem.cuh"
 
@@ -41,6 +42,18 @@ struct Store<__nv_bfloat16> {
     __device__ __forceinline__ static void store(__nv_bfloat16* p, float v, float scale) { *p = __float2bfloat16_rn(v * scale); }
 };
 
+// Per-slice flag bits (one int per slice of a slab).  A set bit only sends
+// work to the fully tested path, so a conservative (sticky) bit is harmless.
+constexpr int kFlagVolEmpty = 1;    // the volume holds a -1e30 voxel (AreTomo's "empty")
+constexpr int kFlagRawLow = 2;      // the staged sinogram holds values <= kLowValue
+constexpr int kFlagDiffLow = 4;     // the residual holds values <= kLowValue
+constexpr float kLowValue = -5.0e9f;  // far from any lerp of values above it reaching -1e10
+
+// y-slices one thread carries: every slice has the same geometry (single
+// tilt axis), so positions, weights, indices and bounds are formed once and
+// only the loads and the accumulation repeat per slice.
+constexpr int SB = 4;
+
 // ---------------------------------------------------------------------------
 // SART staging: raw[ys][t][x] = proj[t][y0 + ys][x] * (cos_t / Nz), x < N.
 // AreTomo/Recon/CDoSartRecon.cpp:100-117 (row gather) and
@@ -48,13 +61,19 @@ struct Store<__nv_bfloat16> {
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(256) k_gather_weight(const float* __restrict__ proj, size_t tilt_stride,
                                                        int row_pitch, int y0, const float2* __restrict__ cs, int T,
-                                                       int N, int Nz, float* __restrict__ raw)
+                                                       int N, int Nz, float* __restrict__ raw, int* __restrict__ flags)
 {
     const int t = blockIdx.x, ys = blockIdx.y;
     const float w = __ldg(&cs[t].x) / (float)Nz;
     const float* src = proj + (size_t)t * tilt_stride + (size_t)(y0 + ys) * row_pitch;
     float* dst = raw + ((size_t)ys * T + t) * N;
-    for (int x = threadIdx.x; x < N; x += blockDim.x) dst[x] = __ldg(src + x) * w;
+    bool low = false;
+    for (int x = threadIdx.x; x < N; x += blockDim.x) {
+        const float v = __ldg(src + x) * w;
+        dst[x] = v;
+        low |= v <= kLowValue;
+    }
+    if (low) atomicOr(flags + ys, kFlagRawLow);
 }
 
 // ---------------------------------------------------------------------------
@@ -66,7 +85,8 @@ __global__ void __launch_bounds__(256) k_gather_weight(const float* __restrict__
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(512) k_rweight(const float* __restrict__ proj, size_t tilt_stride, int row_pitch,
                                                  int y0, const float2* __restrict__ cs, int T, int N, int Nz,
-                                                 const float* __restrict__ hhalf, FftPlan plan, float* __restrict__ out)
+                                                 const float* __restrict__ hhalf, FftPlan plan, float* __restrict__ out,
+                                                 int* __restrict__ flags)
 {
     extern __shared__ float2 fsm[];
     float2* a = fsm;
@@ -89,11 +109,17 @@ __global__ void __launch_bounds__(512) k_rweight(const float* __restrict__ proj,
     __syncthreads();
     float2* r2 = fft_run(r, r == a ? b : a, plan, 1, plan.work, +1);
     float* d0 = out + ((size_t)ys * T + t0) * N;
+    bool low = false;
     for (int x = threadIdx.x; x < N; x += blockDim.x) {
         const float2 v = r2[x];
         d0[x] = v.x;
-        if (two) d0[N + x] = v.y;
+        low |= v.x <= kLowValue;
+        if (two) {
+            d0[N + x] = v.y;
+            low |= v.y <= kLowValue;
+        }
     }
+    if (low) atomicOr(flags + ys, kFlagRawLow);
 }
 
 // ---------------------------------------------------------------------------
@@ -103,12 +129,20 @@ __global__ void __launch_bounds__(512) k_rweight(const float* __restrict__ proj,
 // WBP 2x grid (AreTomo/Recon/GBackProjWbp.cu:14-53): mean over all tilts,
 // or 0 where no tilt contributes.
 //
-// A CTA covers BP_TX x BP_TZ voxels of one slice.  For every tilt it stages
-// in shared memory only the detector window its voxels can reach (the
-// sinogram position is affine in the voxel coordinates, so the window is
-// bounded by the tile's corners).  Voxels are written warp-contiguous in x.
+// A CTA covers BP_TX x BP_TZ voxels of SB slices; each thread keeps 2 x 4
+// voxel positions (x warp-contiguous) for all SB slices.  Tilts go in chunks
+// of BP_CHUNK: for each tilt the CTA stages in shared memory only the
+// detector window its voxels reach (the detector position is affine in the
+// voxel coordinates, so the tile's corners bound it), as (p[i], p[i+1]) pairs
+// so that one 8-byte load feeds a lerp.  Positions, indices, weights and the
+// in-detector test are computed once per voxel and tilt and serve all SB
+// slices; a chunk whose tilts keep the whole tile strictly inside [0, N-2]
+// skips the test.  Slices whose staged data hold values near the -1e10
+// "empty" marker (flag bit) go through the per-slice path that tests every
+// sample as the reference does.  All paths add the same values in the same
+// (tilt) order.
 // ---------------------------------------------------------------------------
-constexpr int BP_TX = 64, BP_TZ = 32, BP_THREADS = 256;
+constexpr int BP_TX = 64, BP_TZ = 32, BP_THREADS = 256, BP_CHUNK = 16;
 constexpr int BP_CX = BP_TX / 32, BP_CZ = BP_TZ / (BP_THREADS / 32);
 
 struct BpArgs {
@@ -116,54 +150,68 @@ struct BpArgs {
     int T, N, t0, t1;
     const float2* cs;
     int GX, GZ;              // voxel grid of this mode
+    int S;                   // slices in this launch
     float relax;
     float* out;              // MODE 0: vol slab [slices][GZ][GX] (z flipped); MODE 1: [slices][GZ][GX]
     size_t out_slice;
-    int ww;                  // staged window width (floats)
-    int* flags;              // MODE 0: per-slice "wrote a sentinel" flag
+    int ww;                  // staged window width (samples)
+    int* flags;              // per-slice flag bits
+    int low_bit;             // the flag bit that marks this sinogram as holding low values
 };
 
 template <int MODE>
 __device__ __forceinline__ float bp_xp(float fX, float fZs, float c, float cent)
 {
     // MODE 0: fX*c + fZ*s + N/2.0f            (GBackProj.cu:35-36)
-    // MODE 1: (fX*c + fZ*s)/2 + (N/2) + 0.5f  (GBackProjWbp.cu:34-35)
+    // MODE 1: (fX*c + fZ*s)/2 + (N/2) + 0.5f  (GBackProjWbp.cu:34-35); a/2 is
+    //         exact, so fl(a/2 + cent) is one fused multiply-add.
     const float a = __fmaf_rn(fX, c, fZs);
     if (MODE == 0) return __fadd_rn(a, cent);
-    return __fadd_rn(__fadd_rn(__fmul_rn(a, 0.5f), cent), 0.5f);
+    return __fadd_rn(__fmaf_rn(a, 0.5f, cent), 0.5f);
+}
+
+__host__ __device__ inline size_t bp_smem_bytes(int ww)
+{
+    return (sizeof(int) + sizeof(float2)) * BP_CHUNK + sizeof(float2) * (size_t)SB * BP_CHUNK * ww;
+}
+
+template <int MODE>
+__device__ __forceinline__ void bp_store(const BpArgs& p, int ys, int Z, int X, float sum, int cnt)
+{
+    float* out = p.out + (size_t)ys * p.out_slice;
+    if (MODE == 0) {
+        if (cnt <= 0) return;
+        float* v = out + (size_t)(p.GZ - 1 - Z) * p.GX + X;
+        const float f = __fadd_rn(__fdiv_rn(__fmul_rn(p.relax, sum), (float)cnt), *v);
+        if (f > kSentinelTest) {
+            *v = fmaxf(f, 0.f);
+        } else {
+            *v = kSentinelValue;
+            atomicOr(p.flags + ys, kFlagVolEmpty);
+        }
+    } else {
+        out[(size_t)Z * p.GX + X] = cnt > 0 ? __fdiv_rn(sum, (float)cnt) : 0.f;
+    }
 }
 
 template <int MODE>
 __global__ void __launch_bounds__(BP_THREADS) k_bp(BpArgs p)
 {
-    extern __shared__ float bsm[];
-    const int nt = p.t1 - p.t0;
-    int* ws = reinterpret_cast<int*>(bsm);
-    float* win = bsm + ((nt + 3) & ~3);
-    const int ys = blockIdx.z, X0 = blockIdx.x * BP_TX, Z0 = blockIdx.y * BP_TZ;
-    const float* sino = p.sino + (size_t)ys * p.T * p.N;
+    extern __shared__ float2 bsm[];
+    float2* cs_s = bsm;                                               // [BP_CHUNK]
+    float2* pw = bsm + BP_CHUNK;                                      // [SB][BP_CHUNK][ww]
+    int* ws = reinterpret_cast<int*>(pw + (size_t)SB * BP_CHUNK * p.ww);  // [BP_CHUNK]
+    const int ys0 = blockIdx.z * SB, nsl = min(SB, p.S - ys0);
+    const int X0 = blockIdx.x * BP_TX, Z0 = blockIdx.y * BP_TZ;
     const float cent = MODE == 0 ? (float)p.N / 2.0f : (float)(p.N / 2);
     const float hx = MODE == 0 ? (float)p.GX * 0.5f : (float)p.GX / 2.0f;
     const float hz = MODE == 0 ? (float)p.GZ * 0.5f : (float)p.GZ / 2.0f;
+    const float endX = (float)(p.N - 2);
+    const unsigned wmax = (unsigned)(p.ww - 2);
+    const size_t pslab = (size_t)BP_CHUNK * p.ww;   // pairs per slice in shared memory
 
-    for (int t = threadIdx.x; t < nt; t += blockDim.x) {
-        const float2 c = __ldg(&p.cs[p.t0 + t]);
-        float lo = 3.0e38f;
-#pragma unroll
-        for (int k = 0; k < 4; k++) {
-            const float fX = (float)(X0 + ((k & 1) ? BP_TX - 1 : 0)) - hx;
-            const float fZ = (float)(Z0 + ((k & 2) ? BP_TZ - 1 : 0)) - hz;
-            lo = fminf(lo, bp_xp<MODE>(fX, __fmul_rn(fZ, c.y), c.x, cent));
-        }
-        ws[t] = (int)floorf(lo) - 1;
-    }
-    __syncthreads();
-    for (int idx = threadIdx.x; idx < nt * p.ww; idx += blockDim.x) {
-        const int t = idx / p.ww, k = idx - t * p.ww;
-        const int x = ws[t] + k;
-        win[idx] = (x >= 0 && x < p.N) ? __ldg(sino + (size_t)(p.t0 + t) * p.N + x) : 0.f;
-    }
-    __syncthreads();
+    bool low = false;
+    for (int q = 0; q < nsl; q++) low |= (__ldg(p.flags + ys0 + q) & p.low_bit) != 0;
 
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     float fX[BP_CX], fZ[BP_CZ];
@@ -171,60 +219,142 @@ __global__ void __launch_bounds__(BP_THREADS) k_bp(BpArgs p)
     for (int i = 0; i < BP_CX; i++) fX[i] = (float)(X0 + lane + 32 * i) - hx;
 #pragma unroll
     for (int j = 0; j < BP_CZ; j++) fZ[j] = (float)(Z0 + warp + (BP_THREADS / 32) * j) - hz;
-    float sum[BP_CZ][BP_CX];
-    int cnt[BP_CZ][BP_CX];
-#pragma unroll
-    for (int j = 0; j < BP_CZ; j++)
-#pragma unroll
-        for (int i = 0; i < BP_CX; i++) { sum[j][i] = 0.f; cnt[j][i] = 0; }
-    const float endX = (float)(p.N - 2);
-    const int wmax = p.ww - 2;
 
-    for (int t = 0; t < nt; t++) {
-        const float2 c = __ldg(&p.cs[p.t0 + t]);
-        const float* w = win + t * p.ww;
-        const int st = ws[t];
+    // stage chunk [c0, c0 + nc) of slices [ys0, ys0 + ns) into pw; returns
+    // whether the whole tile stays strictly inside the detector for it
+    auto stage = [&](int c0, int nc, int ysA, int ns) -> bool {
+        int inside = 1;
+        if (threadIdx.x < nc) {
+            const float2 c = __ldg(&p.cs[c0 + threadIdx.x]);
+            float lo = 3.0e38f, hi = -3.0e38f;
 #pragma unroll
-        for (int j = 0; j < BP_CZ; j++) {
-            const float fzs = __fmul_rn(fZ[j], c.y);
+            for (int k = 0; k < 4; k++) {
+                const float cX = (float)(X0 + ((k & 1) ? BP_TX - 1 : 0)) - hx;
+                const float cZ = (float)(Z0 + ((k & 2) ? BP_TZ - 1 : 0)) - hz;
+                const float xp = bp_xp<MODE>(cX, __fmul_rn(cZ, c.y), c.x, cent);
+                lo = fminf(lo, xp);
+                hi = fmaxf(hi, xp);
+            }
+            ws[threadIdx.x] = (int)floorf(lo) - 1;
+            cs_s[threadIdx.x] = c;
+            inside = (lo >= 0.01f) && (hi <= endX - 0.01f);
+        }
+        inside = __syncthreads_and(inside);
+        const int per = nc * p.ww;
+        for (int idx = threadIdx.x; idx < ns * per; idx += blockDim.x) {
+            const int q = idx / per, r = idx - q * per;
+            const int t = r / p.ww, k = r - t * p.ww;
+            const int x = ws[t] + k;
+            const float* row = p.sino + ((size_t)(ysA + q) * p.T + c0 + t) * p.N;
+            const float a = (x >= 0 && x < p.N) ? __ldg(row + x) : 0.f;
+            const float b = (x + 1 >= 0 && x + 1 < p.N) ? __ldg(row + x + 1) : 0.f;
+            pw[q * pslab + r] = make_float2(a, b);
+        }
+        __syncthreads();
+        return inside != 0;
+    };
+
+    if (!low) {
+        float sum[SB][BP_CZ][BP_CX];
+        int cnt[BP_CZ][BP_CX];
+#pragma unroll
+        for (int j = 0; j < BP_CZ; j++)
 #pragma unroll
             for (int i = 0; i < BP_CX; i++) {
-                const float xp = bp_xp<MODE>(fX[i], fzs, c.x, cent);
-                if (xp >= 0.f && xp <= endX) {
-                    const int ii = (int)xp;
-                    const float fr = __fsub_rn(xp, (float)ii);
-                    const int k = min(max(ii - st, 0), wmax);
-                    const float v = __fmaf_rn(w[k], __fsub_rn(1.f, fr), __fmul_rn(w[k + 1], fr));
-                    if (v > kSentinelTest) {
-                        sum[j][i] = __fadd_rn(sum[j][i], v);
-                        cnt[j][i] += 1;
+                cnt[j][i] = 0;
+#pragma unroll
+                for (int q = 0; q < SB; q++) sum[q][j][i] = 0.f;
+            }
+        for (int c0 = p.t0; c0 < p.t1; c0 += BP_CHUNK) {
+            const int nc = min(BP_CHUNK, p.t1 - c0);
+            const bool inside = stage(c0, nc, ys0, nsl);
+            for (int t = 0; t < nc; t++) {
+                const float2 c = cs_s[t];
+                const float2* w = pw + t * p.ww;
+                const int st = ws[t];
+#pragma unroll
+                for (int j = 0; j < BP_CZ; j++) {
+                    const float fzs = __fmul_rn(fZ[j], c.y);
+#pragma unroll
+                    for (int i = 0; i < BP_CX; i++) {
+                        const float xp = bp_xp<MODE>(fX[i], fzs, c.x, cent);
+                        if (!inside && !(xp >= 0.f && xp <= endX)) continue;
+                        const int ii = (int)xp;
+                        const float fr = __fsub_rn(xp, (float)ii);
+                        const float om = __fsub_rn(1.f, fr);
+                        const float2* wq = w + min((unsigned)(ii - st), wmax);
+#pragma unroll
+                        for (int q = 0; q < SB; q++) {
+                            const float2 v = wq[q * pslab];
+                            sum[q][j][i] = __fadd_rn(sum[q][j][i], __fmaf_rn(v.x, om, __fmul_rn(v.y, fr)));
+                        }
+                        if (!inside) cnt[j][i] += 1;
                     }
                 }
             }
+            if (inside)
+#pragma unroll
+                for (int j = 0; j < BP_CZ; j++)
+#pragma unroll
+                    for (int i = 0; i < BP_CX; i++) cnt[j][i] += nc;
+            __syncthreads();
         }
+#pragma unroll
+        for (int j = 0; j < BP_CZ; j++) {
+            const int Z = Z0 + warp + (BP_THREADS / 32) * j;
+#pragma unroll
+            for (int i = 0; i < BP_CX; i++) {
+                const int X = X0 + lane + 32 * i;
+                if (Z >= p.GZ || X >= p.GX) continue;
+#pragma unroll
+                for (int q = 0; q < SB; q++)
+                    if (q < nsl) bp_store<MODE>(p, ys0 + q, Z, X, sum[q][j][i], cnt[j][i]);
+            }
+        }
+        return;
     }
 
-    float* out = p.out + (size_t)ys * p.out_slice;
+    // per-slice path: every sample tested as the reference does
+    for (int q = 0; q < nsl; q++) {
+        float sum[BP_CZ][BP_CX];
+        int cnt[BP_CZ][BP_CX];
 #pragma unroll
-    for (int j = 0; j < BP_CZ; j++) {
-        const int Z = Z0 + warp + (BP_THREADS / 32) * j;
-        if (Z >= p.GZ) continue;
+        for (int j = 0; j < BP_CZ; j++)
 #pragma unroll
-        for (int i = 0; i < BP_CX; i++) {
-            const int X = X0 + lane + 32 * i;
-            if (X >= p.GX) continue;
-            if (MODE == 0) {
-                if (cnt[j][i] <= 0) continue;
-                float* v = out + (size_t)(p.GZ - 1 - Z) * p.GX + X;
-                const float f = __fadd_rn(__fdiv_rn(__fmul_rn(p.relax, sum[j][i]), (float)cnt[j][i]), *v);
-                if (f > kSentinelTest) {
-                    *v = fmaxf(f, 0.f);
-                } else {
-                    *v = kSentinelValue;
-                    p.flags[ys] = 1;
+            for (int i = 0; i < BP_CX; i++) { sum[j][i] = 0.f; cnt[j][i] = 0; }
+        for (int c0 = p.t0; c0 < p.t1; c0 += BP_CHUNK) {
+            const int nc = min(BP_CHUNK, p.t1 - c0);
+            stage(c0, nc, ys0 + q, 1);
+            for (int t = 0; t < nc; t++) {
+                const float2 c = cs_s[t];
+                const float2* w = pw + t * p.ww;
+                const int st = ws[t];
+#pragma unroll
+                for (int j = 0; j < BP_CZ; j++) {
+                    const float fzs = __fmul_rn(fZ[j], c.y);
+#pragma unroll
+                    for (int i = 0; i < BP_CX; i++) {
+                        const float xp = bp_xp<MODE>(fX[i], fzs, c.x, cent);
+                        const int ii = (int)xp;
+                        const float fr = __fsub_rn(xp, (float)ii);
+                        const float2 v2 = w[min((unsigned)(ii - st), wmax)];
+                        const float v = __fmaf_rn(v2.x, __fsub_rn(1.f, fr), __fmul_rn(v2.y, fr));
+                        if (xp >= 0.f && xp <= endX && v > kSentinelTest) {
+                            sum[j][i] = __fadd_rn(sum[j][i], v);
+                            cnt[j][i] += 1;
+                        }
+                    }
                 }
-            } else {
-                out[(size_t)Z * p.GX + X] = cnt[j][i] > 0 ? __fdiv_rn(sum[j][i], (float)cnt[j][i]) : 0.f;
+            }
+            __syncthreads();
+        }
+#pragma unroll
+        for (int j = 0; j < BP_CZ; j++) {
+            const int Z = Z0 + warp + (BP_THREADS / 32) * j;
+#pragma unroll
+            for (int i = 0; i < BP_CX; i++) {
+                const int X = X0 + lane + 32 * i;
+                if (Z < p.GZ && X < p.GX) bp_store<MODE>(p, ys0 + q, Z, X, sum[j][i], cnt[j][i]);
             }
         }
     }
@@ -235,56 +365,155 @@ __global__ void __launch_bounds__(BP_THREADS) k_bp(BpArgs p)
 // AreTomo/Recon/GForProj.cu:10-76 (ray of L = int(Nz/cos + 1.5) samples,
 // bilinear, mean over in-volume samples, -1e30 if none) followed by
 // AreTomo/Recon/GDiffProj.cu:7-21 (d = raw - fp, 0 where either is empty).
-// One ray per thread; a warp walks 32 neighbouring rays in lock-step, so each
-// step reads two short runs of two volume rows.  Optional residual sums for
-// the per-iteration R-factor are reduced per CTA and added in FP64.
-// Grid (ceil(N/256), tilts, slices).
+// One ray per thread, for SB slices at once; the lanes of a warp are
+// neighbouring rays and step through sample index i in lock-step, so every
+// step reads two short runs of two volume rows per slice.
+//
+// The sample positions x_i = fma(-z0_i, sin, tx), z_i = fma(z0_i, cos, tz)
+// (z0_i = i - L/2) are monotonic in i after FP32 rounding too, so the samples
+// the reference keeps (0 <= x <= Nx-2, 0 <= z <= Nz-2) form one contiguous
+// range of i per ray.  Each ray finds that range exactly (an estimate, then
+// a walk to the first/last index that passes the reference's own test) and
+// samples it without per-sample bounds tests; positions and weights serve
+// all SB slices.  Slices whose volume may hold "empty" voxels (flag bit) are
+// projected one at a time with the per-sample value test kept.
+// Grid (ceil(N/256), tilts, ceil(slices/SB)).
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) k_fp_diff(const float* __restrict__ vol, int Nx, int Nz,
+struct RayPos {
+    float tx, tz, c, s, halfL;
+    __device__ __forceinline__ float x(int i) const { return __fmaf_rn(-((float)i - halfL), s, tx); }
+    __device__ __forceinline__ float z(int i) const { return __fmaf_rn((float)i - halfL, c, tz); }
+};
+
+// First index in [lo, hi + 1] where a predicate that is monotonic false -> true
+// over [lo, hi] holds, starting the walk from an estimate.
+template <class P>
+__device__ __forceinline__ int first_true(int lo, int hi, int est, P pred)
+{
+    est = min(max(est, lo), hi + 1);
+    while (est > lo && pred(est - 1)) est--;
+    while (est <= hi && !pred(est)) est++;
+    return est;
+}
+
+__device__ __forceinline__ int est_index(float v) { return (int)fminf(fmaxf(v, -1.0e8f), 1.0e8f); }
+
+// Ray set-up: position of ray u of tilt (c, s), and the in-volume sample
+// range [lo, hi] (empty when lo > hi).
+__device__ __forceinline__ void fp_ray_setup(int u, int N, int Nx, int Nz, float c, float s, RayPos& r, int& lo,
+                                             int& hi)
+{
+    r.c = c;
+    r.s = s;
+    const int L = (int)((float)Nz / c + 1.5f);
+    const float fXp = (float)u - 0.5f * (float)N;
+    r.tx = fXp / c + (float)Nx * 0.5f;
+    r.tz = (float)Nz * 0.5f;
+    r.halfL = (float)L * 0.5f;
+    const float endX = (float)(Nx - 2), endZ = (float)(Nz - 2);
+    lo = first_true(0, L - 1, est_index(ceilf(r.halfL - r.tz / c)), [&](int i) { return r.z(i) >= 0.f; });
+    hi = first_true(lo, L - 1, est_index(floorf(r.halfL + (endZ - r.tz) / c)) + 1,
+                    [&](int i) { return r.z(i) > endZ; }) - 1;
+    if (s > 0.f) {
+        lo = first_true(lo, hi, est_index(ceilf(r.halfL + (r.tx - endX) / s)), [&](int i) { return r.x(i) <= endX; });
+        hi = first_true(lo, hi, est_index(floorf(r.halfL + r.tx / s)) + 1, [&](int i) { return r.x(i) < 0.f; }) - 1;
+    } else if (s < 0.f) {
+        lo = first_true(lo, hi, est_index(ceilf(r.halfL + r.tx / s)), [&](int i) { return r.x(i) >= 0.f; });
+        hi = first_true(lo, hi, est_index(floorf(r.halfL + (r.tx - endX) / s)) + 1,
+                        [&](int i) { return r.x(i) > endX; }) - 1;
+    } else if (!(r.tx >= 0.f && r.tx <= endX)) {
+        hi = lo - 1;
+    }
+}
+
+__device__ __forceinline__ float bilerp(float a00, float a10, float a01, float a11, float wx, float wz)
+{
+    const float A = __fmaf_rn(wz, a01 - a00, a00);
+    const float B = __fmaf_rn(wz, a11 - a10, a10);
+    return __fmaf_rn(wx, B - A, A);
+}
+
+__global__ void __launch_bounds__(256) k_fp_diff(const float* __restrict__ vol, int Nx, int Nz, int S,
                                                  const float* __restrict__ raw, float* __restrict__ diff,
                                                  const float2* __restrict__ cs, int T, int N, int t0,
-                                                 double* __restrict__ rf)
+                                                 double* __restrict__ rf, int* __restrict__ flags)
 {
     const int u = blockIdx.x * blockDim.x + threadIdx.x;
-    const int t = t0 + blockIdx.y, ys = blockIdx.z;
-    float ad = 0.f, ar = 0.f;
-    if (u < N) {
-        const float2 c = __ldg(&cs[t]);
-        const float fCos = c.x, fSin = c.y;
-        const int L = (int)((float)Nz / fCos + 1.5f);
-        const float fXp = (float)u - 0.5f * (float)N;
-        const float fTempX = fXp / fCos + (float)Nx * 0.5f;
-        const float fTempZ = (float)Nz * 0.5f;
-        const float halfL = (float)L * 0.5f;
-        const float endX = (float)(Nx - 2), endZ = (float)(Nz - 2);
-        // the volume slab is stored z flipped: voxel (X, Z) at row Nz-1-Z
-        const float* v0 = vol + (size_t)ys * Nx * Nz + (size_t)(Nz - 1) * Nx;
-        float fSum = 0.f, fCount = 0.f;
-        for (int i = 0; i < L; i++) {
-            const float z0 = (float)i - halfL;
-            const float fX = __fmaf_rn(-z0, fSin, fTempX);
-            const float fZ = __fmaf_rn(z0, fCos, fTempZ);
-            if (fX < 0.f || fZ < 0.f || fX > endX || fZ > endZ) continue;
+    const int t = t0 + blockIdx.y, ys0 = blockIdx.z * SB, nsl = min(SB, S - ys0);
+    const bool active = u < N;
+    const float2 cc = __ldg(&cs[t]);
+    RayPos r;
+    int lo, hi;
+    fp_ray_setup(active ? u : N - 1, N, Nx, Nz, cc.x, cc.y, r, lo, hi);
+    if (!active) { lo = 1; hi = 0; }
+    // the warp walks one common index range so its lanes read the same rows
+    const int wlo = __reduce_min_sync(0xffffffffu, lo <= hi ? lo : INT_MAX);
+    const int whi = __reduce_max_sync(0xffffffffu, lo <= hi ? hi : INT_MIN);
+    const size_t slice = (size_t)Nx * Nz;
+    const float* vbase = vol + (size_t)(Nz - 1) * Nx;   // voxel (X, Z) at row Nz-1-Z
+    bool empty_vox = false;
+    for (int q = 0; q < nsl; q++) empty_vox |= (__ldg(flags + ys0 + q) & kFlagVolEmpty) != 0;
+
+    float fSum[SB], fCount[SB];
+#pragma unroll
+    for (int q = 0; q < SB; q++) { fSum[q] = 0.f; fCount[q] = 0.f; }
+    if (!empty_vox) {
+        const float* vq[SB];
+#pragma unroll
+        for (int q = 0; q < SB; q++) vq[q] = vbase + (size_t)(ys0 + min(q, nsl - 1)) * slice;
+        for (int i = wlo; i <= whi; i++) {
+            if (i < lo || i > hi) continue;
+            const float fX = r.x(i), fZ = r.z(i);
             const int iX = (int)fX, iZ = (int)fZ;
             const float wx = fX - (float)iX, wz = fZ - (float)iZ;
-            const float* q = v0 - (size_t)iZ * Nx + iX;
-            const float a00 = __ldg(q), a10 = __ldg(q + 1), a01 = __ldg(q - Nx), a11 = __ldg(q - Nx + 1);
-            const float val = a00 * (1.f - wx) * (1.f - wz) + a10 * wx * (1.f - wz) + a01 * (1.f - wx) * wz +
-                              a11 * wx * wz;
-            if (val < kSentinelTest) continue;
-            fSum += val;
-            fCount += 1.f;
+            const ptrdiff_t o = iX - (ptrdiff_t)iZ * Nx;
+#pragma unroll
+            for (int q = 0; q < SB; q++) {
+                const float* p = vq[q] + o;
+                fSum[q] += bilerp(__ldg(p), __ldg(p + 1), __ldg(p - Nx), __ldg(p - Nx + 1), wx, wz);
+            }
         }
-        const float fp = fCount <= 0.f ? kSentinelValue : fSum / fCount;
-        const size_t o = ((size_t)ys * T + t) * N + u;
-        const float r = __ldg(raw + o);
-        float d = 0.f;
-        if (!(fp < kSentinelTest) && !(r < kSentinelTest)) {
-            d = r - fp;
-            ad = fabsf(d);
-            ar = fabsf(r);
+        const float n = (float)max(hi - lo + 1, 0);
+#pragma unroll
+        for (int q = 0; q < SB; q++) fCount[q] = n;
+    } else {
+        for (int q = 0; q < nsl; q++) {
+            const float* v0 = vbase + (size_t)(ys0 + q) * slice;
+            float s0 = 0.f, n0 = 0.f;
+            for (int i = wlo; i <= whi; i++) {
+                if (i < lo || i > hi) continue;
+                const float fX = r.x(i), fZ = r.z(i);
+                const int iX = (int)fX, iZ = (int)fZ;
+                const float* p = v0 + iX - (ptrdiff_t)iZ * Nx;
+                const float val = bilerp(__ldg(p), __ldg(p + 1), __ldg(p - Nx), __ldg(p - Nx + 1), fX - (float)iX,
+                                         fZ - (float)iZ);
+                if (val < kSentinelTest) continue;
+                s0 += val;
+                n0 += 1.f;
+            }
+#pragma unroll
+            for (int k = 0; k < SB; k++)
+                if (k == q) { fSum[k] = s0; fCount[k] = n0; }
         }
-        diff[o] = d;
+    }
+
+    float ad = 0.f, ar = 0.f;
+    if (active) {
+#pragma unroll
+        for (int q = 0; q < SB; q++) {
+            if (q >= nsl) continue;
+            const float fp = fCount[q] <= 0.f ? kSentinelValue : fSum[q] / fCount[q];
+            const size_t o = ((size_t)(ys0 + q) * T + t) * N + u;
+            const float rw = __ldg(raw + o);
+            float d = 0.f;
+            if (!(fp < kSentinelTest) && !(rw < kSentinelTest)) {
+                d = rw - fp;
+                ad += fabsf(d);
+                ar += fabsf(rw);
+                if (d <= kLowValue) atomicOr(flags + ys0 + q, kFlagDiffLow);
+            }
+            diff[o] = d;
+        }
     }
     if (rf) {
 #pragma unroll
@@ -298,7 +527,7 @@ __global__ void __launch_bounds__(256) k_fp_diff(const float* __restrict__ vol, 
         __syncthreads();
         if (threadIdx.x == 0) {
             double sd = 0, sr = 0;
-            for (int k = 0; k < (int)(blockDim.x >> 5); k++) { sd += red[0][k]; sr += red[1][k]; }
+            for (int k = 0; k < 8; k++) { sd += red[0][k]; sr += red[1][k]; }
             atomicAdd(rf, sd);
             atomicAdd(rf + 1, sr);
         }
@@ -316,7 +545,7 @@ __global__ void __launch_bounds__(256) k_fill_empty(float* __restrict__ vol, siz
                                                     const int* __restrict__ flags)
 {
     const int ys = blockIdx.x;
-    if (flags[ys] == 0) return;
+    if ((flags[ys] & kFlagVolEmpty) == 0) return;
     float* v = vol + (size_t)ys * slice_elems;
     float s = 0.f, n = 0.f;
     for (size_t i = threadIdx.x; i < slice_elems; i += blockDim.x)

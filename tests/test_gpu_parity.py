@@ -170,6 +170,20 @@ def test_sart_edge_parameters_vs_oracle(R, start, num, iters, subsets):
     assert rel_l2(out, o64) < ORACLE_TOL
 
 
+@pytest.mark.parametrize("nx,lim", [(98, 60), (128, 78)])
+def test_sart_l1_forward_projector_cases_vs_oracle(R, nx, lim):
+    """Nx = 98 (not a multiple of 4, no TMA volume map) and tilts to +-78
+    degrees (rays too oblique for one TMA tile) use the L1 forward projector."""
+    tilts = np.linspace(-lim, lim, 27).astype(np.float32)
+    frames = _series(nx, 3, tilts, 36, seed=nx + lim, noise=2)
+    meta = dict(mode="sart", vol_z=36, start=0, ntilts=27, iters=2, subsets=3)
+    out = ours(R, frames, tilts, meta)
+    o64 = sart(frames, tilts, 36, 0, 27, 2, 3)
+    err = rel_l2(out, o64)
+    print(f"SART nx={nx} tilts +-{lim}: rel-L2 vs FP64 oracle {err:.3e}")
+    assert err < ORACLE_TOL
+
+
 def test_sart_rfactor_decreases_and_matches_oracle(R):
     from aretomo3_b200 import synth
     tilts = synth.tilt_range(-60, 60, 4)
