@@ -283,13 +283,17 @@ size_t bp_smem(int, int ww) { return bp_smem_bytes(ww); }
 // coexist; the amount a launch uses is still its own.
 at3r_status set_smem(const void* fn, size_t bytes)
 {
-    constexpr size_t kMax = 227 * 1024;
+    int dev = 0, optin = 0;
+    AT3R_CUDA(cudaGetDevice(&dev));
+    AT3R_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+    cudaFuncAttributes fa{};
+    AT3R_CUDA(cudaFuncGetAttributes(&fa, fn));
+    const size_t kMax = (size_t)optin - fa.sharedSizeBytes;   // dynamic part the kernel may ask for
     if (bytes > kMax)
-        return set_err(AT3R_ERR_TOO_LARGE, "shared-memory need " + std::to_string(bytes) + " exceeds 227 KB");
+        return set_err(AT3R_ERR_TOO_LARGE, "shared-memory need " + std::to_string(bytes) + " exceeds " +
+                                               std::to_string(kMax) + " bytes");
     static std::mutex mu;
     static std::map<std::pair<const void*, int>, bool> done;
-    int dev = 0;
-    cudaGetDevice(&dev);
     std::lock_guard<std::mutex> lk(mu);
     if (!done[{fn, dev}]) {
         AT3R_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMax));
@@ -378,8 +382,8 @@ at3r_status run_slab(at3r_plan* p, const float* proj, size_t tilt_stride, int pr
                 for (int t = t0; t < t0 + nt; t++) samples += (double)p->ray_len[t];
                 double* rfp = p->g.compute_rfactor ? p->d_rf + 2 * it : nullptr;
                 TB(p, st);
-                k_fp_diff<<<dim3((N + 255) / 256, nt, SG), 256, 0, st>>>(vol, Nx, Nz, S, p->d_raw, p->d_diff,
-                                                                         p->d_cs, T, N, t0, rfp, p->d_flags);
+                k_fp_diff<<<dim3((N + 255) / 256, nt, SG), 256, 0, st>>>(vol, Nx, Nz, S, p->d_raw, p->d_diff, p->d_cs,
+                                                                         T, N, t0, rfp, p->d_flags);
                 TE(p, st, KK_FP_DIFF, f4 * (vox + 2.0 * S * nt * N), samples * N * S);
                 a.t0 = t0; a.t1 = t0 + nt;
                 TB(p, st);

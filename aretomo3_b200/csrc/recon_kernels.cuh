@@ -240,15 +240,18 @@ __global__ void __launch_bounds__(BP_THREADS) k_bp(BpArgs p)
             inside = (lo >= 0.01f) && (hi <= endX - 0.01f);
         }
         inside = __syncthreads_and(inside);
-        const int per = nc * p.ww;
-        for (int idx = threadIdx.x; idx < ns * per; idx += blockDim.x) {
-            const int q = idx / per, r = idx - q * per;
-            const int t = r / p.ww, k = r - t * p.ww;
-            const int x = ws[t] + k;
-            const float* row = p.sino + ((size_t)(ysA + q) * p.T + c0 + t) * p.N;
-            const float a = (x >= 0 && x < p.N) ? __ldg(row + x) : 0.f;
-            const float b = (x + 1 >= 0 && x + 1 < p.N) ? __ldg(row + x + 1) : 0.f;
-            pw[q * pslab + r] = make_float2(a, b);
+        // one warp per (slice, tilt) row, lanes along the window
+        for (int row = warp; row < ns * nc; row += BP_THREADS / 32) {
+            const int q = row / nc, t = row - q * nc;
+            const int x0 = ws[t];
+            const float* src = p.sino + ((size_t)(ysA + q) * p.T + c0 + t) * p.N;
+            float2* dst = pw + q * pslab + t * p.ww;
+            for (int k = lane; k < p.ww; k += 32) {
+                const int x = x0 + k;
+                const float a = (x >= 0 && x < p.N) ? __ldg(src + x) : 0.f;
+                const float b = (x + 1 >= 0 && x + 1 < p.N) ? __ldg(src + x + 1) : 0.f;
+                dst[k] = make_float2(a, b);
+            }
         }
         __syncthreads();
         return inside != 0;
@@ -268,35 +271,61 @@ __global__ void __launch_bounds__(BP_THREADS) k_bp(BpArgs p)
         for (int c0 = p.t0; c0 < p.t1; c0 += BP_CHUNK) {
             const int nc = min(BP_CHUNK, p.t1 - c0);
             const bool inside = stage(c0, nc, ys0, nsl);
-            for (int t = 0; t < nc; t++) {
-                const float2 c = cs_s[t];
-                const float2* w = pw + t * p.ww;
-                const int st = ws[t];
+            if (inside) {
+                // the whole tile lands inside the detector for every tilt of the chunk
+                for (int t = 0; t < nc; t++) {
+                    const float2 c = cs_s[t];
+                    const float2* w = pw + t * p.ww;
+                    const int st = ws[t];
 #pragma unroll
-                for (int j = 0; j < BP_CZ; j++) {
-                    const float fzs = __fmul_rn(fZ[j], c.y);
+                    for (int j = 0; j < BP_CZ; j++) {
+                        const float fzs = __fmul_rn(fZ[j], c.y);
 #pragma unroll
-                    for (int i = 0; i < BP_CX; i++) {
-                        const float xp = bp_xp<MODE>(fX[i], fzs, c.x, cent);
-                        if (!inside && !(xp >= 0.f && xp <= endX)) continue;
-                        const int ii = (int)xp;
-                        const float fr = __fsub_rn(xp, (float)ii);
-                        const float om = __fsub_rn(1.f, fr);
-                        const float2* wq = w + min((unsigned)(ii - st), wmax);
+                        for (int i = 0; i < BP_CX; i++) {
+                            const float xp = bp_xp<MODE>(fX[i], fzs, c.x, cent);
+                            const int ii = (int)xp;
+                            const float fr = __fsub_rn(xp, (float)ii);
+                            const float om = __fsub_rn(1.f, fr);
+                            const float2* wq = w + min((unsigned)(ii - st), wmax);
 #pragma unroll
-                        for (int q = 0; q < SB; q++) {
-                            const float2 v = wq[q * pslab];
-                            sum[q][j][i] = __fadd_rn(sum[q][j][i], __fmaf_rn(v.x, om, __fmul_rn(v.y, fr)));
+                            for (int q = 0; q < SB; q++) {
+                                const float2 v = wq[q * pslab];
+                                sum[q][j][i] = __fadd_rn(sum[q][j][i], __fmaf_rn(v.x, om, __fmul_rn(v.y, fr)));
+                            }
                         }
-                        if (!inside) cnt[j][i] += 1;
                     }
                 }
-            }
-            if (inside)
 #pragma unroll
                 for (int j = 0; j < BP_CZ; j++)
 #pragma unroll
                     for (int i = 0; i < BP_CX; i++) cnt[j][i] += nc;
+            } else {
+                for (int t = 0; t < nc; t++) {
+                    const float2 c = cs_s[t];
+                    const float2* w = pw + t * p.ww;
+                    const int st = ws[t];
+#pragma unroll
+                    for (int j = 0; j < BP_CZ; j++) {
+                        const float fzs = __fmul_rn(fZ[j], c.y);
+#pragma unroll
+                        for (int i = 0; i < BP_CX; i++) {
+                            const float xp = bp_xp<MODE>(fX[i], fzs, c.x, cent);
+                            const bool in = xp >= 0.f && xp <= endX;
+                            const int ii = (int)xp;
+                            const float fr = __fsub_rn(xp, (float)ii);
+                            const float om = __fsub_rn(1.f, fr);
+                            const float2* wq = w + min((unsigned)(ii - st), wmax);
+#pragma unroll
+                            for (int q = 0; q < SB; q++) {
+                                const float2 v = wq[q * pslab];
+                                const float add = __fmaf_rn(v.x, om, __fmul_rn(v.y, fr));
+                                sum[q][j][i] = in ? __fadd_rn(sum[q][j][i], add) : sum[q][j][i];
+                            }
+                            cnt[j][i] += in ? 1 : 0;
+                        }
+                    }
+                }
+            }
             __syncthreads();
         }
 #pragma unroll

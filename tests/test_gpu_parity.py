@@ -170,10 +170,9 @@ def test_sart_edge_parameters_vs_oracle(R, start, num, iters, subsets):
     assert rel_l2(out, o64) < ORACLE_TOL
 
 
-@pytest.mark.parametrize("nx,lim", [(98, 60), (128, 78)])
-def test_sart_l1_forward_projector_cases_vs_oracle(R, nx, lim):
-    """Nx = 98 (not a multiple of 4, no TMA volume map) and tilts to +-78
-    degrees (rays too oblique for one TMA tile) use the L1 forward projector."""
+@pytest.mark.parametrize("nx,lim", [(98, 60), (128, 78), (128, 85)])
+def test_sart_oblique_and_odd_width_vs_oracle(R, nx, lim):
+    """An odd-by-2 width and steep tilts (long, strongly sheared rays)."""
     tilts = np.linspace(-lim, lim, 27).astype(np.float32)
     frames = _series(nx, 3, tilts, 36, seed=nx + lim, noise=2)
     meta = dict(mode="sart", vol_z=36, start=0, ntilts=27, iters=2, subsets=3)
