@@ -469,6 +469,8 @@ at3r_status at3r_plan_create(const at3r_geom* g, at3r_plan** out)
     *out = nullptr;
     if (g->nx < 4 || g->ny < 1 || g->n_tilts < 1 || g->vol_z < 2 || !g->tilts_deg)
         return set_err(AT3R_ERR_INVALID_ARGUMENT, "sizes must satisfy nx >= 4, ny >= 1, n_tilts >= 1, vol_z >= 2");
+    if ((long long)(g->nx & ~1) * g->vol_z * 4 >= (1LL << 31))
+        return set_err(AT3R_ERR_TOO_LARGE, "(nx & ~1) * vol_z must stay below 2^29 (32-bit in-slice offsets)");
     if (g->method != AT3R_WBP && g->method != AT3R_SART)
         return set_err(AT3R_ERR_INVALID_ARGUMENT, "method must be AT3R_WBP or AT3R_SART");
     if (g->storage != AT3R_STORE_F32)
@@ -522,6 +524,7 @@ at3r_status at3r_plan_create(const at3r_geom* g, at3r_plan** out)
         for (int i = 0; i < n % k; i++) p->sub_size[i]++;
         for (int i = 1; i < k; i++) p->sub_start[i] = p->sub_start[i - 1] + p->sub_size[i - 1];
         p->bp_ww_sart = bp_window(BP_TX, BP_TZ, 1.0, cs, p->T);
+        if (p->bp_ww_sart > BP_WW) return fail(set_err(AT3R_ERR_TOO_LARGE, "back-projection window exceeds its stride"));
         if ((rc = set_smem((const void*)k_bp<0>, bp_smem(p->T, p->bp_ww_sart)))) return fail(rc);
         per_slice = 2 * T * N * sizeof(float) + Nx * Nz * sizeof(float);
     } else {
@@ -539,6 +542,7 @@ at3r_status at3r_plan_create(const at3r_geom* g, at3r_plan** out)
         while (p->zcrop_cb > 1 && 2 * sizeof(float2) * p->zcrop_cb * p->zcrop_pitch > 227 * 1024) p->zcrop_cb /= 2;
         p->smem_zcrop = 2 * sizeof(float2) * p->zcrop_cb * p->zcrop_pitch;
         p->bp_ww_wbp = bp_window(BP_TX, BP_TZ, 0.5, cs, p->T);
+        if (p->bp_ww_wbp > BP_WW) return fail(set_err(AT3R_ERR_TOO_LARGE, "back-projection window exceeds its stride"));
         if ((rc = set_smem((const void*)k_rweight, p->smem_rweight))) return fail(rc);
         if ((rc = set_smem((const void*)k_row_r2c, p->smem_row))) return fail(rc);
         if ((rc = set_smem((const void*)k_zcrop, p->smem_zcrop))) return fail(rc);
@@ -792,6 +796,8 @@ extern "C" at3r_status at3r_sart_device_noalloc(const float* proj, int nx, int n
         return set_err(AT3R_ERR_INVALID_ARGUMENT, "SART needs subsets >= 1 and iterations >= 0");
     if (start_tilt < 0 || num_tilts < 0 || start_tilt + num_tilts > n_tilts)
         return set_err(AT3R_ERR_INVALID_ARGUMENT, "SART tilt range outside the series");
+    if ((long long)(nx & ~1) * vol_z * 4 >= (1LL << 31))
+        return set_err(AT3R_ERR_TOO_LARGE, "(nx & ~1) * vol_z must stay below 2^29 (32-bit in-slice offsets)");
     const int T = n_tilts, N = nx & ~1, Nx = N, Nz = vol_z;
     if (T > kNoallocMaxTilts)
         return set_err(AT3R_ERR_TOO_LARGE, "the no-allocation entry point takes at most " +
@@ -812,6 +818,7 @@ extern "C" at3r_status at3r_sart_device_noalloc(const float* proj, int nx, int n
             return set_err(AT3R_ERR_INVALID_ARGUMENT, "tilt angles must satisfy |tilt| < 89.9 degrees");
     }
     const int ww = bp_window(BP_TX, BP_TZ, 1.0, cs, T);
+    if (ww > BP_WW) return set_err(AT3R_ERR_TOO_LARGE, "back-projection window exceeds its stride");
     if (bp_smem(T, ww) > 227 * 1024) return set_err(AT3R_ERR_TOO_LARGE, "back-projection window exceeds 227 KB");
     unsigned char* base = nullptr;
     at3r_status rc = noalloc_scratch_address(&base);

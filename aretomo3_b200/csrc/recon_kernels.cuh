@@ -143,6 +143,11 @@ __global__ void __launch_bounds__(512) k_rweight(const float* __restrict__ proj,
 // (tilt) order.
 // ---------------------------------------------------------------------------
 constexpr int BP_TX = 64, BP_TZ = 32, BP_THREADS = 256, BP_CHUNK = 16;
+// Shared-memory stride of one tilt's staged window (pairs).  A window spans
+// at most (BP_TX - 1) + (BP_TZ - 1) + 6 = 100 samples (|cos|, |sin| <= 1), so
+// a fixed stride holds every case and makes the per-slice offsets immediates.
+constexpr int BP_WW = 128;
+constexpr int BP_PSLAB = BP_CHUNK * BP_WW;   // pairs per slice
 constexpr int BP_CX = BP_TX / 32, BP_CZ = BP_TZ / (BP_THREADS / 32);
 
 struct BpArgs {
@@ -170,9 +175,9 @@ __device__ __forceinline__ float bp_xp(float fX, float fZs, float c, float cent)
     return __fadd_rn(__fmaf_rn(a, 0.5f, cent), 0.5f);
 }
 
-__host__ __device__ inline size_t bp_smem_bytes(int ww)
+__host__ __device__ inline size_t bp_smem_bytes(int)
 {
-    return (sizeof(int) + sizeof(float2)) * BP_CHUNK + sizeof(float2) * (size_t)SB * BP_CHUNK * ww;
+    return (sizeof(int) + sizeof(float2)) * BP_CHUNK + sizeof(float2) * (size_t)SB * BP_PSLAB;
 }
 
 template <int MODE>
@@ -199,8 +204,8 @@ __global__ void __launch_bounds__(BP_THREADS) k_bp(BpArgs p)
 {
     extern __shared__ float2 bsm[];
     float2* cs_s = bsm;                                               // [BP_CHUNK]
-    float2* pw = bsm + BP_CHUNK;                                      // [SB][BP_CHUNK][ww]
-    int* ws = reinterpret_cast<int*>(pw + (size_t)SB * BP_CHUNK * p.ww);  // [BP_CHUNK]
+    float2* pw = bsm + BP_CHUNK;                                      // [SB][BP_CHUNK][BP_WW]
+    int* ws = reinterpret_cast<int*>(pw + SB * BP_PSLAB);             // [BP_CHUNK]
     const int ys0 = blockIdx.z * SB, nsl = min(SB, p.S - ys0);
     const int X0 = blockIdx.x * BP_TX, Z0 = blockIdx.y * BP_TZ;
     const float cent = MODE == 0 ? (float)p.N / 2.0f : (float)(p.N / 2);
@@ -208,7 +213,6 @@ __global__ void __launch_bounds__(BP_THREADS) k_bp(BpArgs p)
     const float hz = MODE == 0 ? (float)p.GZ * 0.5f : (float)p.GZ / 2.0f;
     const float endX = (float)(p.N - 2);
     const unsigned wmax = (unsigned)(p.ww - 2);
-    const size_t pslab = (size_t)BP_CHUNK * p.ww;   // pairs per slice in shared memory
 
     bool low = false;
     for (int q = 0; q < nsl; q++) low |= (__ldg(p.flags + ys0 + q) & p.low_bit) != 0;
@@ -245,7 +249,7 @@ __global__ void __launch_bounds__(BP_THREADS) k_bp(BpArgs p)
             const int q = row / nc, t = row - q * nc;
             const int x0 = ws[t];
             const float* src = p.sino + ((size_t)(ysA + q) * p.T + c0 + t) * p.N;
-            float2* dst = pw + q * pslab + t * p.ww;
+            float2* dst = pw + q * BP_PSLAB + t * BP_WW;
             for (int k = lane; k < p.ww; k += 32) {
                 const int x = x0 + k;
                 const float a = (x >= 0 && x < p.N) ? __ldg(src + x) : 0.f;
@@ -275,7 +279,7 @@ __global__ void __launch_bounds__(BP_THREADS) k_bp(BpArgs p)
                 // the whole tile lands inside the detector for every tilt of the chunk
                 for (int t = 0; t < nc; t++) {
                     const float2 c = cs_s[t];
-                    const float2* w = pw + t * p.ww;
+                    const float2* w = pw + t * BP_WW;
                     const int st = ws[t];
 #pragma unroll
                     for (int j = 0; j < BP_CZ; j++) {
@@ -289,7 +293,7 @@ __global__ void __launch_bounds__(BP_THREADS) k_bp(BpArgs p)
                             const float2* wq = w + min((unsigned)(ii - st), wmax);
 #pragma unroll
                             for (int q = 0; q < SB; q++) {
-                                const float2 v = wq[q * pslab];
+                                const float2 v = wq[q * BP_PSLAB];
                                 sum[q][j][i] = __fadd_rn(sum[q][j][i], __fmaf_rn(v.x, om, __fmul_rn(v.y, fr)));
                             }
                         }
@@ -302,7 +306,7 @@ __global__ void __launch_bounds__(BP_THREADS) k_bp(BpArgs p)
             } else {
                 for (int t = 0; t < nc; t++) {
                     const float2 c = cs_s[t];
-                    const float2* w = pw + t * p.ww;
+                    const float2* w = pw + t * BP_WW;
                     const int st = ws[t];
 #pragma unroll
                     for (int j = 0; j < BP_CZ; j++) {
@@ -317,7 +321,7 @@ __global__ void __launch_bounds__(BP_THREADS) k_bp(BpArgs p)
                             const float2* wq = w + min((unsigned)(ii - st), wmax);
 #pragma unroll
                             for (int q = 0; q < SB; q++) {
-                                const float2 v = wq[q * pslab];
+                                const float2 v = wq[q * BP_PSLAB];
                                 const float add = __fmaf_rn(v.x, om, __fmul_rn(v.y, fr));
                                 sum[q][j][i] = in ? __fadd_rn(sum[q][j][i], add) : sum[q][j][i];
                             }
@@ -356,7 +360,7 @@ __global__ void __launch_bounds__(BP_THREADS) k_bp(BpArgs p)
             stage(c0, nc, ys0 + q, 1);
             for (int t = 0; t < nc; t++) {
                 const float2 c = cs_s[t];
-                const float2* w = pw + t * p.ww;
+                const float2* w = pw + t * BP_WW;
                 const int st = ws[t];
 #pragma unroll
                 for (int j = 0; j < BP_CZ; j++) {
@@ -487,19 +491,26 @@ __global__ void __launch_bounds__(256) k_fp_diff(const float* __restrict__ vol, 
 #pragma unroll
     for (int q = 0; q < SB; q++) { fSum[q] = 0.f; fCount[q] = 0.f; }
     if (!empty_vox) {
-        const float* vq[SB];
+        // per slice, the rows of voxel Z and Z + 1 as loop-invariant bases; a
+        // sample then costs one 32-bit cell offset and one wide add per row
+        const float* r0[SB];
+        const float* r1[SB];
 #pragma unroll
-        for (int q = 0; q < SB; q++) vq[q] = vbase + (size_t)(ys0 + min(q, nsl - 1)) * slice;
+        for (int q = 0; q < SB; q++) {
+            r0[q] = vbase + (size_t)(ys0 + min(q, nsl - 1)) * slice;
+            r1[q] = r0[q] - Nx;
+        }
         for (int i = wlo; i <= whi; i++) {
             if (i < lo || i > hi) continue;
             const float fX = r.x(i), fZ = r.z(i);
             const int iX = (int)fX, iZ = (int)fZ;
             const float wx = fX - (float)iX, wz = fZ - (float)iZ;
-            const ptrdiff_t o = iX - (ptrdiff_t)iZ * Nx;
+            const int o = iX - iZ * Nx;   // within one slice: |o| < Nx * Nz
 #pragma unroll
             for (int q = 0; q < SB; q++) {
-                const float* p = vq[q] + o;
-                fSum[q] += bilerp(__ldg(p), __ldg(p + 1), __ldg(p - Nx), __ldg(p - Nx + 1), wx, wz);
+                const float* p0 = r0[q] + o;
+                const float* p1 = r1[q] + o;
+                fSum[q] += bilerp(__ldg(p0), __ldg(p0 + 1), __ldg(p1), __ldg(p1 + 1), wx, wz);
             }
         }
         const float n = (float)max(hi - lo + 1, 0);
