@@ -221,15 +221,19 @@ struct at3r_plan {
     float relax = 1.f;
     std::vector<int> sub_start, sub_size;
     float2* d_cs = nullptr;
+    // staged sinograms: element size by storage type; row scales for 16-bit storage
+    size_t esz = sizeof(float);
+    float* d_scale = nullptr;
     // SART
-    float* d_raw = nullptr;
-    float* d_diff = nullptr;
+    void* d_raw = nullptr;
+    void* d_diff = nullptr;
+    void* d_shadow = nullptr;   // 16-bit storage: the volume shadow the forward projector reads
     int* d_flags = nullptr;
     double* d_rf = nullptr;
     std::vector<double> h_rf;
     // WBP
     float* d_h = nullptr;
-    float* d_filt = nullptr;
+    void* d_filt = nullptr;
     float* d_g2 = nullptr;    // also holds the cropped spectrum w
     float2* d_y = nullptr;
     HostFft fN, f2x, f2z, fz, fx;
@@ -259,6 +263,17 @@ at3r_status dalloc(at3r_plan* p, T** ptr, size_t count)
 {
     const size_t bytes = count * sizeof(T);
     cudaError_t e = cudaMalloc((void**)ptr, bytes);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return set_err(AT3R_ERR_OUT_OF_MEMORY, "cudaMalloc of " + std::to_string(bytes) + " bytes failed");
+    }
+    p->ws_bytes += bytes;
+    return AT3R_OK;
+}
+
+at3r_status dalloc_bytes(at3r_plan* p, void** ptr, size_t bytes)
+{
+    cudaError_t e = cudaMalloc(ptr, bytes);
     if (e != cudaSuccess) {
         cudaGetLastError();
         return set_err(AT3R_ERR_OUT_OF_MEMORY, "cudaMalloc of " + std::to_string(bytes) + " bytes failed");
@@ -351,29 +366,37 @@ at3r_status tend(at3r_plan* p, cudaStream_t st, int kind, double bytes, double u
 // One slab of slices [y0, y0 + S): proj points at tilt 0 row 0 of a
 // [T][rows][nx] block whose row `proj_y0` is slice y0; vol points at the
 // slab's first output slice.
-at3r_status run_slab(at3r_plan* p, const float* proj, size_t tilt_stride, int proj_y0, int S, float* vol,
-                     cudaStream_t st)
+template <typename ST, typename VT>
+at3r_status run_slab_t(at3r_plan* p, const float* proj, size_t tilt_stride, int proj_y0, int S, float* vol,
+                       cudaStream_t st)
 {
+    ST* raw = static_cast<ST*>(p->d_raw);
+    ST* dif = static_cast<ST*>(p->d_diff);
+    ST* filt = static_cast<ST*>(p->d_filt);
+    const double es = (double)sizeof(ST), vs = std::is_same<VT, float>::value ? 4.0 : 2.0;
     const int T = p->T, N = p->N, Nx = p->Nx, Nz = p->Nz, KX = p->KX;
     const double f4 = 4.0, vox = (double)S * Nx * Nz;
     const int SG = (S + SB - 1) / SB;   // slice groups: each thread carries SB slices
     AT3R_CUDA(cudaMemsetAsync(p->d_flags, 0, sizeof(int) * S, st));
     if (p->g.method == AT3R_SART) {
         TB(p, st);
-        k_gather_weight<<<dim3(T, S), 256, 0, st>>>(proj, tilt_stride, p->nx, proj_y0, p->d_cs, T, N, Nz, p->d_raw,
-                                                    p->d_flags);
-        TE(p, st, KK_GATHER, 2 * f4 * S * T * N, (double)S * T * N);
+        k_gather_weight<ST><<<dim3(T, S), 256, 0, st>>>(proj, tilt_stride, p->nx, proj_y0, p->d_cs, T, N, Nz, raw,
+                                                        p->d_scale, p->d_flags);
+        TE(p, st, KK_GATHER, (f4 + es) * S * T * N, (double)S * T * N);
         AT3R_CUDA(cudaMemsetAsync(vol, 0, sizeof(float) * (size_t)S * Nx * Nz, st));
+        if (p->d_shadow)
+            AT3R_CUDA(cudaMemsetAsync(p->d_shadow, 0, 2 * (size_t)((S + 1) & ~1) * Nx * Nz, st));
         BpArgs a{};
         a.T = T; a.N = N; a.cs = p->d_cs; a.GX = Nx; a.GZ = Nz; a.S = S;
         a.out = vol; a.out_slice = (size_t)Nx * Nz; a.ww = p->bp_ww_sart; a.flags = p->d_flags;
+        a.scale = p->d_scale; a.shadow = p->d_shadow;
         const dim3 bgrid((Nx + BP_TX - 1) / BP_TX, (Nz + BP_TZ - 1) / BP_TZ, SG);
         // first back-projection: all tilts, relax 1 (CTomoSart.cpp:68-69)
-        a.sino = p->d_raw; a.t0 = 0; a.t1 = T; a.relax = 1.f; a.low_bit = kFlagRawLow;
+        a.sino = raw; a.t0 = 0; a.t1 = T; a.relax = 1.f; a.low_bit = kFlagRawLow;
         TB(p, st);
-        k_bp<0><<<bgrid, BP_THREADS, bp_smem(T, a.ww), st>>>(a);
-        TE(p, st, KK_BP_SART, f4 * (S * (double)T * N + 2 * vox), vox * T);
-        a.sino = p->d_diff; a.relax = p->relax; a.low_bit = kFlagDiffLow;
+        k_bp<0, ST, VT><<<bgrid, BP_THREADS, bp_smem(T, a.ww), st>>>(a);
+        TE(p, st, KK_BP_SART, es * S * (double)T * N + (2 * f4 + (vs < 4 ? vs : 0)) * vox, vox * T);
+        a.sino = dif; a.relax = p->relax; a.low_bit = kFlagDiffLow;
         for (int it = 0; it < p->g.iterations; it++) {
             for (size_t s = 0; s < p->sub_start.size(); s++) {
                 const int t0 = p->sub_start[s] + p->g.start_tilt, nt = p->sub_size[s];
@@ -382,13 +405,13 @@ at3r_status run_slab(at3r_plan* p, const float* proj, size_t tilt_stride, int pr
                 for (int t = t0; t < t0 + nt; t++) samples += (double)p->ray_len[t];
                 double* rfp = p->g.compute_rfactor ? p->d_rf + 2 * it : nullptr;
                 TB(p, st);
-                k_fp_diff<<<dim3((N + 255) / 256, nt, SG), 256, 0, st>>>(vol, Nx, Nz, S, p->d_raw, p->d_diff, p->d_cs,
-                                                                         T, N, t0, rfp, p->d_flags);
-                TE(p, st, KK_FP_DIFF, f4 * (vox + 2.0 * S * nt * N), samples * N * S);
+                k_fp_diff<ST, VT><<<dim3((N + 255) / 256, nt, SG), 256, 0, st>>>(
+                    vol, p->d_shadow, Nx, Nz, S, raw, dif, p->d_scale, p->d_cs, T, N, t0, rfp, p->d_flags);
+                TE(p, st, KK_FP_DIFF, vs * vox + 2.0 * es * S * nt * N, samples * N * S);
                 a.t0 = t0; a.t1 = t0 + nt;
                 TB(p, st);
-                k_bp<0><<<bgrid, BP_THREADS, bp_smem(nt, a.ww), st>>>(a);
-                TE(p, st, KK_BP_SART, f4 * (S * (double)nt * N + 2 * vox), vox * nt);
+                k_bp<0, ST, VT><<<bgrid, BP_THREADS, bp_smem(nt, a.ww), st>>>(a);
+                TE(p, st, KK_BP_SART, es * S * (double)nt * N + (2 * f4 + (vs < 4 ? vs : 0)) * vox, vox * nt);
             }
         }
         TB(p, st);
@@ -398,17 +421,18 @@ at3r_status run_slab(at3r_plan* p, const float* proj, size_t tilt_stride, int pr
     }
     // WBP
     TB(p, st);
-    k_rweight<<<dim3((T + 1) / 2, S), 512, p->smem_rweight, st>>>(proj, tilt_stride, p->nx, proj_y0, p->d_cs, T, N,
-                                                                  Nz, p->d_h, p->fN.plan, p->d_filt, p->d_flags);
-    TE(p, st, KK_RWEIGHT, 2 * f4 * S * T * N, (double)S * T * N);
+    k_rweight<ST><<<dim3((T + 1) / 2, S), 512, p->smem_rweight, st>>>(proj, tilt_stride, p->nx, proj_y0, p->d_cs, T,
+                                                                      N, Nz, p->d_h, p->fN.plan, filt, p->d_scale,
+                                                                      p->d_flags);
+    TE(p, st, KK_RWEIGHT, (f4 + es) * S * T * N, (double)S * T * N);
     BpArgs a{};
-    a.sino = p->d_filt; a.T = T; a.N = N; a.t0 = 0; a.t1 = T; a.cs = p->d_cs;
+    a.sino = filt; a.scale = p->d_scale; a.shadow = nullptr; a.T = T; a.N = N; a.t0 = 0; a.t1 = T; a.cs = p->d_cs;
     a.GX = 2 * Nx; a.GZ = 2 * Nz; a.S = S; a.relax = 1.f; a.out = p->d_g2; a.out_slice = (size_t)4 * Nx * Nz;
     a.ww = p->bp_ww_wbp; a.flags = p->d_flags; a.low_bit = kFlagRawLow;
     const dim3 bgrid((2 * Nx + BP_TX - 1) / BP_TX, (2 * Nz + BP_TZ - 1) / BP_TZ, SG);
     TB(p, st);
-    k_bp<1><<<bgrid, BP_THREADS, bp_smem(T, a.ww), st>>>(a);
-    TE(p, st, KK_BP_WBP, f4 * (S * (double)T * N + 4 * vox), 4 * vox * T);
+    k_bp<1, ST, float><<<bgrid, BP_THREADS, bp_smem(T, a.ww), st>>>(a);
+    TE(p, st, KK_BP_WBP, es * S * (double)T * N + f4 * 4 * vox, 4 * vox * T);
     TB(p, st);
     k_row_r2c<<<dim3(Nz, S), 512, p->smem_row, st>>>(p->d_g2, Nx, Nz, p->f2x.plan, p->d_y);
     TE(p, st, KK_ROW_R2C, f4 * 4 * vox + 8.0 * S * 2 * Nz * KX, 4 * vox);
@@ -423,6 +447,17 @@ at3r_status run_slab(at3r_plan* p, const float* proj, size_t tilt_stride, int pr
                                                               (size_t)Nx * Nz);
     TE(p, st, KK_XC2R, 8.0 * S * Nz * KX + f4 * vox, vox);
     return AT3R_OK;
+}
+
+at3r_status run_slab(at3r_plan* p, const float* proj, size_t tilt_stride, int proj_y0, int S, float* vol,
+                     cudaStream_t st)
+{
+    switch (p->g.storage) {
+        case AT3R_STORE_F16: return run_slab_t<__half, __half>(p, proj, tilt_stride, proj_y0, S, vol, st);
+        case AT3R_STORE_BF16:
+            return run_slab_t<__nv_bfloat16, __nv_bfloat16>(p, proj, tilt_stride, proj_y0, S, vol, st);
+        default: return run_slab_t<float, float>(p, proj, tilt_stride, proj_y0, S, vol, st);
+    }
 }
 
 at3r_status begin_run(at3r_plan* p, cudaStream_t st)
@@ -473,8 +508,8 @@ at3r_status at3r_plan_create(const at3r_geom* g, at3r_plan** out)
         return set_err(AT3R_ERR_TOO_LARGE, "(nx & ~1) * vol_z must stay below 2^29 (32-bit in-slice offsets)");
     if (g->method != AT3R_WBP && g->method != AT3R_SART)
         return set_err(AT3R_ERR_INVALID_ARGUMENT, "method must be AT3R_WBP or AT3R_SART");
-    if (g->storage != AT3R_STORE_F32)
-        return set_err(AT3R_ERR_UNSUPPORTED, "reduced-precision storage is not available in this build");
+    if (g->storage != AT3R_STORE_F32 && g->storage != AT3R_STORE_F16 && g->storage != AT3R_STORE_BF16)
+        return set_err(AT3R_ERR_INVALID_ARGUMENT, "storage must be AT3R_STORE_F32, _F16 or _BF16");
     if (g->method == AT3R_SART) {
         if (g->subsets < 1 || g->iterations < 0)
             return set_err(AT3R_ERR_INVALID_ARGUMENT, "SART needs subsets >= 1 and iterations >= 0");
@@ -488,6 +523,7 @@ at3r_status at3r_plan_create(const at3r_geom* g, at3r_plan** out)
     }
     at3r_plan* p = new at3r_plan();
     p->g = *g;
+    p->esz = g->storage == AT3R_STORE_F32 ? sizeof(float) : 2;
     p->tilts.assign(g->tilts_deg, g->tilts_deg + g->n_tilts);
     p->g.tilts_deg = p->tilts.data();
     p->nx = g->nx; p->ny = g->ny; p->T = g->n_tilts;
@@ -525,7 +561,9 @@ at3r_status at3r_plan_create(const at3r_geom* g, at3r_plan** out)
         for (int i = 1; i < k; i++) p->sub_start[i] = p->sub_start[i - 1] + p->sub_size[i - 1];
         p->bp_ww_sart = bp_window(BP_TX, BP_TZ, 1.0, cs, p->T);
         if (p->bp_ww_sart > BP_WW) return fail(set_err(AT3R_ERR_TOO_LARGE, "back-projection window exceeds its stride"));
-        if ((rc = set_smem((const void*)k_bp<0>, bp_smem(p->T, p->bp_ww_sart)))) return fail(rc);
+        for (const void* fn : {(const void*)k_bp<0, float, float>, (const void*)k_bp<0, __half, __half>,
+                               (const void*)k_bp<0, __nv_bfloat16, __nv_bfloat16>})
+            if ((rc = set_smem(fn, bp_smem(p->T, p->bp_ww_sart)))) return fail(rc);
         per_slice = 2 * T * N * sizeof(float) + Nx * Nz * sizeof(float);
     } else {
         p->c2r = g->c2r == AT3R_C2R_MATCH_CUFFT ? probe_cufft_c2r(p->Nz, p->Nx) : g->c2r;
@@ -543,11 +581,15 @@ at3r_status at3r_plan_create(const at3r_geom* g, at3r_plan** out)
         p->smem_zcrop = 2 * sizeof(float2) * p->zcrop_cb * p->zcrop_pitch;
         p->bp_ww_wbp = bp_window(BP_TX, BP_TZ, 0.5, cs, p->T);
         if (p->bp_ww_wbp > BP_WW) return fail(set_err(AT3R_ERR_TOO_LARGE, "back-projection window exceeds its stride"));
-        if ((rc = set_smem((const void*)k_rweight, p->smem_rweight))) return fail(rc);
+        for (const void* fn : {(const void*)k_rweight<float>, (const void*)k_rweight<__half>,
+                               (const void*)k_rweight<__nv_bfloat16>})
+            if ((rc = set_smem(fn, p->smem_rweight))) return fail(rc);
         if ((rc = set_smem((const void*)k_row_r2c, p->smem_row))) return fail(rc);
         if ((rc = set_smem((const void*)k_zcrop, p->smem_zcrop))) return fail(rc);
         if ((rc = set_smem((const void*)k_x_c2r, p->smem_xc2r))) return fail(rc);
-        if ((rc = set_smem((const void*)k_bp<1>, bp_smem(p->T, p->bp_ww_wbp)))) return fail(rc);
+        for (const void* fn : {(const void*)k_bp<1, float, float>, (const void*)k_bp<1, __half, float>,
+                               (const void*)k_bp<1, __nv_bfloat16, float>})
+            if ((rc = set_smem(fn, bp_smem(p->T, p->bp_ww_wbp)))) return fail(rc);
         // R-weight transfer function (GRWeight.cu:15-20), 1/N folded in
         std::vector<float> h(N / 2 + 1);
         const double twopi = (double)6.2831852f;
@@ -570,13 +612,19 @@ at3r_status at3r_plan_create(const at3r_geom* g, at3r_plan** out)
     p->slab = std::min(slab, p->ny);
     const size_t S = p->slab;
     if (g->method == AT3R_SART) {
-        if ((rc = dalloc(p, &p->d_raw, S * T * N))) return fail(rc);
-        if ((rc = dalloc(p, &p->d_diff, S * T * N))) return fail(rc);
+        if ((rc = dalloc_bytes(p, &p->d_raw, S * T * N * p->esz))) return fail(rc);
+        if ((rc = dalloc_bytes(p, &p->d_diff, S * T * N * p->esz))) return fail(rc);
+        if (g->storage != AT3R_STORE_F32) {
+            if ((rc = dalloc(p, &p->d_scale, S * T))) return fail(rc);
+            // slice pairs of 16-bit values, the slab rounded up to whole SB groups
+            if ((rc = dalloc_bytes(p, &p->d_shadow, 2 * ((S + SB - 1) / SB * SB) * Nx * Nz))) return fail(rc);
+        }
         if ((rc = dalloc(p, &p->d_flags, S))) return fail(rc);
         if ((rc = dalloc(p, &p->d_rf, 2 * (size_t)std::max(1, g->iterations)))) return fail(rc);
         p->h_rf.assign(2 * std::max(1, g->iterations), 0.0);
     } else {
-        if ((rc = dalloc(p, &p->d_filt, S * T * N))) return fail(rc);
+        if ((rc = dalloc_bytes(p, &p->d_filt, S * T * N * p->esz))) return fail(rc);
+        if (g->storage != AT3R_STORE_F32 && (rc = dalloc(p, &p->d_scale, S * T))) return fail(rc);
         if ((rc = dalloc(p, &p->d_flags, S))) return fail(rc);
         if ((rc = dalloc(p, &p->d_g2, S * 4 * Nx * Nz))) return fail(rc);
         if ((rc = dalloc(p, &p->d_y, S * 2 * Nz * KX))) return fail(rc);
@@ -588,7 +636,7 @@ at3r_status at3r_plan_create(const at3r_geom* g, at3r_plan** out)
 void at3r_plan_destroy(at3r_plan* p)
 {
     if (!p) return;
-    cudaFree(p->d_cs); cudaFree(p->d_raw); cudaFree(p->d_diff); cudaFree(p->d_flags); cudaFree(p->d_rf);
+    cudaFree(p->d_cs); cudaFree(p->d_raw); cudaFree(p->d_diff); cudaFree(p->d_scale); cudaFree(p->d_shadow); cudaFree(p->d_flags); cudaFree(p->d_rf);
     cudaFree(p->d_h); cudaFree(p->d_filt); cudaFree(p->d_g2); cudaFree(p->d_y);
     for (HostFft* f : {&p->fN, &p->f2x, &p->f2z, &p->fz, &p->fx}) cudaFree(f->d_tables);
     for (int i = 0; i < 2; i++) { cudaFree(p->d_proj_slab[i]); cudaFree(p->d_vol_slab[i]); }
@@ -776,7 +824,7 @@ at3r_status noalloc_scratch_address(unsigned char** out)
         return set_err(AT3R_ERR_CUDA, std::string("cudaGetSymbolAddress(no-allocation scratch): ") +
                                           cudaGetErrorString(e));
     }
-    at3r_status rc = set_smem((const void*)k_bp<0>, 0);
+    at3r_status rc = set_smem((const void*)k_bp<0, float, float>, 0);
     if (rc != AT3R_OK) return rc;
     addr[dev] = (unsigned char*)ptr;
     *out = (unsigned char*)ptr;
@@ -842,7 +890,8 @@ extern "C" at3r_status at3r_sart_device_noalloc(const float* proj, int nx, int n
         float* v = vol + (size_t)y0 * Nx * Nz;
         const int SG = (S + SB - 1) / SB;
         AT3R_CUDA(cudaMemsetAsync(d_flags, 0, sizeof(int) * S, st));
-        k_gather_weight<<<dim3(T, S), 256, 0, st>>>(proj, tilt_stride, nx, y0, d_cs, T, N, Nz, d_raw, d_flags);
+        k_gather_weight<float><<<dim3(T, S), 256, 0, st>>>(proj, tilt_stride, nx, y0, d_cs, T, N, Nz, d_raw, nullptr,
+                                                           d_flags);
         AT3R_CUDA(cudaGetLastError());
         AT3R_CUDA(cudaMemsetAsync(v, 0, sizeof(float) * (size_t)S * Nx * Nz, st));
         BpArgs a{};
@@ -850,18 +899,19 @@ extern "C" at3r_status at3r_sart_device_noalloc(const float* proj, int nx, int n
         a.out = v; a.out_slice = (size_t)Nx * Nz; a.ww = ww; a.flags = d_flags;
         const dim3 bgrid((Nx + BP_TX - 1) / BP_TX, (Nz + BP_TZ - 1) / BP_TZ, SG);
         a.sino = d_raw; a.t0 = 0; a.t1 = T; a.relax = 1.f; a.low_bit = kFlagRawLow;
-        k_bp<0><<<bgrid, BP_THREADS, bp_smem(T, ww), st>>>(a);
+        k_bp<0, float, float><<<bgrid, BP_THREADS, bp_smem(T, ww), st>>>(a);
         AT3R_CUDA(cudaGetLastError());
         a.sino = d_diff; a.relax = rlx; a.low_bit = kFlagDiffLow;
         for (int it = 0; it < iterations; it++) {
             for (int s = 0; s < subsets; s++) {
                 const int t0 = sub_start[s] + start_tilt, nt = sub_size[s];
                 if (nt <= 0) continue;
-                k_fp_diff<<<dim3((N + 255) / 256, nt, SG), 256, 0, st>>>(v, Nx, Nz, S, d_raw, d_diff, d_cs, T, N,
-                                                                         t0, nullptr, d_flags);
+                k_fp_diff<float, float><<<dim3((N + 255) / 256, nt, SG), 256, 0, st>>>(v, nullptr, Nx, Nz, S, d_raw, d_diff,
+                                                                                       nullptr, d_cs, T, N, t0, nullptr,
+                                                                                       d_flags);
                 AT3R_CUDA(cudaGetLastError());
                 a.t0 = t0; a.t1 = t0 + nt;
-                k_bp<0><<<bgrid, BP_THREADS, bp_smem(nt, ww), st>>>(a);
+                k_bp<0, float, float><<<bgrid, BP_THREADS, bp_smem(nt, ww), st>>>(a);
                 AT3R_CUDA(cudaGetLastError());
             }
         }

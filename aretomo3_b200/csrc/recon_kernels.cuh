@@ -13,6 +13,7 @@
 #include <cuda_bf16.h>
 #include <stdint.h>
 #include <climits>
+#include <type_traits>
 
 #include "fft_smem.cuh"
 
@@ -22,25 +23,75 @@ constexpr float kSentinelTest = -1e10f;   // "empty sample" threshold of the ref
 constexpr float kSentinelValue = -1e30f;  // value the reference writes for "no sample"
 
 // ---------------------------------------------------------------------------
-// Storage of staged sinograms: FP32, or FP16/BF16 with a per-row scale.
+// Storage of staged sinograms.  FP32 as is; FP16 / BF16 as value / scale with
+// one scale per (slice, tilt) row (the row's largest magnitude), so a row
+// spans [-1, 1] whatever its level.  Accumulation is always FP32.
 // ---------------------------------------------------------------------------
-template <typename S>
-struct Store;
+template <typename ST>
+struct Stor;
 template <>
-struct Store<float> {
-    __device__ __forceinline__ static float load(const float* p, float) { return *p; }
-    __device__ __forceinline__ static void store(float* p, float v, float) { *p = v; }
+struct Stor<float> {
+    __device__ __forceinline__ static float ld(const float* p, float) { return __ldg(p); }
+    __device__ __forceinline__ static void st(float* p, float v, float) { *p = v; }
+};
+// An empty value is stored as NaN, which no stored number equals; it reads
+// back as the reference's -1e30 (a lerp with a zero weight then stays exact).
+__device__ __forceinline__ float unscale(float x, float scale) { return x != x ? kSentinelValue : x * scale; }
+
+template <>
+struct Stor<__half> {
+    __device__ __forceinline__ static float ld(const __half* p, float scale) { return unscale(__half2float(__ldg(p)), scale); }
+    __device__ __forceinline__ static void st(__half* p, float v, float inv)
+    {
+        *p = __float2half_rn(v <= kSentinelTest ? __int_as_float(0x7fc00000) : v * inv);
+    }
 };
 template <>
-struct Store<__half> {
-    __device__ __forceinline__ static float load(const __half* p, float inv) { return __half2float(*p) * inv; }
-    __device__ __forceinline__ static void store(__half* p, float v, float scale) { *p = __float2half_rn(v * scale); }
+struct Stor<__nv_bfloat16> {
+    __device__ __forceinline__ static float ld(const __nv_bfloat16* p, float scale)
+    {
+        return unscale(__bfloat162float(__ldg(p)), scale);
+    }
+    __device__ __forceinline__ static void st(__nv_bfloat16* p, float v, float inv)
+    {
+        *p = __float2bfloat16_rn(v <= kSentinelTest ? __int_as_float(0x7fc00000) : v * inv);
+    }
+};
+
+// Two slices of the 16-bit volume shadow the forward projector reads.
+template <typename VT>
+struct Pair;
+template <>
+struct Pair<__half> {
+    using T2 = __half2;
+    __device__ __forceinline__ static float2 ld(const __half2* p) { return __half22float2(__ldg(p)); }
+    __device__ __forceinline__ static __half2 make(float a, float b) { return __floats2half2_rn(a, b); }
+    __device__ __forceinline__ static __half one(float a) { return __float2half_rn(a); }
 };
 template <>
-struct Store<__nv_bfloat16> {
-    __device__ __forceinline__ static float load(const __nv_bfloat16* p, float inv) { return __bfloat162float(*p) * inv; }
-    __device__ __forceinline__ static void store(__nv_bfloat16* p, float v, float scale) { *p = __float2bfloat16_rn(v * scale); }
+struct Pair<__nv_bfloat16> {
+    using T2 = __nv_bfloat162;
+    __device__ __forceinline__ static float2 ld(const __nv_bfloat162* p) { return __bfloat1622float2(__ldg(p)); }
+    __device__ __forceinline__ static __nv_bfloat162 make(float a, float b) { return __floats2bfloat162_rn(a, b); }
+    __device__ __forceinline__ static __nv_bfloat16 one(float a) { return __float2bfloat16_rn(a); }
 };
+
+// Largest magnitude over a CTA's values (non-empty ones only); every thread
+// gets the result.  Uses red[32] of shared memory.
+__device__ __forceinline__ float block_absmax(float v, float* red)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    __syncthreads();
+    if (lane == 0) red[warp] = v;
+    __syncthreads();
+    float m = 0.f;
+    for (int k = 0; k < (int)((blockDim.x + 31) >> 5); k++) m = fmaxf(m, red[k]);
+    return m;
+}
+
+__device__ __forceinline__ float row_scale(float absmax) { return absmax > 0.f ? absmax : 1.f; }
 
 // Per-slice flag bits (one int per slice of a slab).  A set bit only sends
 // work to the fully tested path, so a conservative (sticky) bit is harmless.
@@ -59,18 +110,32 @@ constexpr int SB = 4;
 // AreTomo/Recon/CDoSartRecon.cpp:100-117 (row gather) and
 // AreTomo/Recon/GWeightProjs.cu:7-19 (weight).  Grid (T, slices).
 // ---------------------------------------------------------------------------
+template <typename ST>
 __global__ void __launch_bounds__(256) k_gather_weight(const float* __restrict__ proj, size_t tilt_stride,
                                                        int row_pitch, int y0, const float2* __restrict__ cs, int T,
-                                                       int N, int Nz, float* __restrict__ raw, int* __restrict__ flags)
+                                                       int N, int Nz, ST* __restrict__ raw, float* __restrict__ scale,
+                                                       int* __restrict__ flags)
 {
     const int t = blockIdx.x, ys = blockIdx.y;
     const float w = __ldg(&cs[t].x) / (float)Nz;
     const float* src = proj + (size_t)t * tilt_stride + (size_t)(y0 + ys) * row_pitch;
-    float* dst = raw + ((size_t)ys * T + t) * N;
+    ST* dst = raw + ((size_t)ys * T + t) * N;
     bool low = false;
+    float inv = 1.f;
+    if constexpr (!std::is_same<ST, float>::value) {
+        __shared__ float red[32];
+        float m = 0.f;
+        for (int x = threadIdx.x; x < N; x += blockDim.x) {
+            const float v = __ldg(src + x) * w;
+            if (v > kSentinelTest) m = fmaxf(m, fabsf(v));
+        }
+        const float sc = row_scale(block_absmax(m, red));
+        inv = 1.f / sc;
+        if (threadIdx.x == 0) scale[(size_t)ys * T + t] = sc;
+    }
     for (int x = threadIdx.x; x < N; x += blockDim.x) {
         const float v = __ldg(src + x) * w;
-        dst[x] = v;
+        Stor<ST>::st(dst + x, v, inv);
         low |= v <= kLowValue;
     }
     if (low) atomicOr(flags + ys, kFlagRawLow);
@@ -83,10 +148,11 @@ __global__ void __launch_bounds__(256) k_gather_weight(const float* __restrict__
 // AreTomo/Recon/GWeightProjs.cu:18, GRWeight.cu:7-23 (+ MaUtil/GFFT1D.cu R2C/C2R).
 // Grid (ceil(T/2), slices).
 // ---------------------------------------------------------------------------
+template <typename ST>
 __global__ void __launch_bounds__(512) k_rweight(const float* __restrict__ proj, size_t tilt_stride, int row_pitch,
                                                  int y0, const float2* __restrict__ cs, int T, int N, int Nz,
-                                                 const float* __restrict__ hhalf, FftPlan plan, float* __restrict__ out,
-                                                 int* __restrict__ flags)
+                                                 const float* __restrict__ hhalf, FftPlan plan, ST* __restrict__ out,
+                                                 float* __restrict__ scale, int* __restrict__ flags)
 {
     extern __shared__ float2 fsm[];
     float2* a = fsm;
@@ -108,14 +174,32 @@ __global__ void __launch_bounds__(512) k_rweight(const float* __restrict__ proj,
     }
     __syncthreads();
     float2* r2 = fft_run(r, r == a ? b : a, plan, 1, plan.work, +1);
-    float* d0 = out + ((size_t)ys * T + t0) * N;
+    ST* d0 = out + ((size_t)ys * T + t0) * N;
+    float inv0 = 1.f, inv1 = 1.f;
+    if constexpr (!std::is_same<ST, float>::value) {
+        __shared__ float red[32];
+        float m0 = 0.f, m1 = 0.f;
+        for (int x = threadIdx.x; x < N; x += blockDim.x) {
+            const float2 v = r2[x];
+            if (v.x > kSentinelTest) m0 = fmaxf(m0, fabsf(v.x));
+            if (v.y > kSentinelTest) m1 = fmaxf(m1, fabsf(v.y));
+        }
+        const float s0 = row_scale(block_absmax(m0, red));
+        const float s1 = row_scale(block_absmax(m1, red));
+        inv0 = 1.f / s0;
+        inv1 = 1.f / s1;
+        if (threadIdx.x == 0) {
+            scale[(size_t)ys * T + t0] = s0;
+            if (two) scale[(size_t)ys * T + t0 + 1] = s1;
+        }
+    }
     bool low = false;
     for (int x = threadIdx.x; x < N; x += blockDim.x) {
         const float2 v = r2[x];
-        d0[x] = v.x;
+        Stor<ST>::st(d0 + x, v.x, inv0);
         low |= v.x <= kLowValue;
         if (two) {
-            d0[N + x] = v.y;
+            Stor<ST>::st(d0 + N + x, v.y, inv1);
             low |= v.y <= kLowValue;
         }
     }
@@ -151,7 +235,8 @@ constexpr int BP_PSLAB = BP_CHUNK * BP_WW;   // pairs per slice
 constexpr int BP_CX = BP_TX / 32, BP_CZ = BP_TZ / (BP_THREADS / 32);
 
 struct BpArgs {
-    const float* sino;       // [slices][T][N]
+    const void* sino;        // [slices][T][N] of the storage type
+    const float* scale;      // [slices][T] row scales (16-bit storage), else null
     int T, N, t0, t1;
     const float2* cs;
     int GX, GZ;              // voxel grid of this mode
@@ -162,6 +247,7 @@ struct BpArgs {
     int ww;                  // staged window width (samples)
     int* flags;              // per-slice flag bits
     int low_bit;             // the flag bit that marks this sinogram as holding low values
+    void* shadow;            // MODE 0, 16-bit volume type: [ceil(slices/2)][GZ][GX] slice pairs (z flipped)
 };
 
 template <int MODE>
@@ -180,26 +266,47 @@ __host__ __device__ inline size_t bp_smem_bytes(int)
     return (sizeof(int) + sizeof(float2)) * BP_CHUNK + sizeof(float2) * (size_t)SB * BP_PSLAB;
 }
 
+// Writes one voxel and returns its value afterwards (the old value where no
+// tilt contributed).
 template <int MODE>
-__device__ __forceinline__ void bp_store(const BpArgs& p, int ys, int Z, int X, float sum, int cnt)
+__device__ __forceinline__ float bp_store(const BpArgs& p, int ys, int Z, int X, float sum, int cnt)
 {
     float* out = p.out + (size_t)ys * p.out_slice;
     if (MODE == 0) {
-        if (cnt <= 0) return;
         float* v = out + (size_t)(p.GZ - 1 - Z) * p.GX + X;
+        if (cnt <= 0) return *v;
         const float f = __fadd_rn(__fdiv_rn(__fmul_rn(p.relax, sum), (float)cnt), *v);
         if (f > kSentinelTest) {
-            *v = fmaxf(f, 0.f);
-        } else {
-            *v = kSentinelValue;
-            atomicOr(p.flags + ys, kFlagVolEmpty);
+            const float r = fmaxf(f, 0.f);
+            *v = r;
+            return r;
         }
+        *v = kSentinelValue;
+        atomicOr(p.flags + ys, kFlagVolEmpty);
+        return kSentinelValue;
     } else {
-        out[(size_t)Z * p.GX + X] = cnt > 0 ? __fdiv_rn(sum, (float)cnt) : 0.f;
+        const float r = cnt > 0 ? __fdiv_rn(sum, (float)cnt) : 0.f;
+        out[(size_t)Z * p.GX + X] = r;
+        return r;
     }
 }
 
-template <int MODE>
+// The 16-bit shadow of the SART volume: slices (2g, 2g+1) share one word.
+template <typename VT>
+__device__ __forceinline__ void shadow_pair(const BpArgs& p, int ys, int Z, int X, float a, float b)
+{
+    using T2 = typename Pair<VT>::T2;
+    T2* sh = reinterpret_cast<T2*>(p.shadow) + ((size_t)(ys >> 1) * p.GZ + (p.GZ - 1 - Z)) * p.GX + X;
+    *sh = Pair<VT>::make(a, b);
+}
+template <typename VT>
+__device__ __forceinline__ void shadow_one(const BpArgs& p, int ys, int Z, int X, float a)
+{
+    VT* sh = reinterpret_cast<VT*>(p.shadow) + 2 * (((size_t)(ys >> 1) * p.GZ + (p.GZ - 1 - Z)) * p.GX + X) + (ys & 1);
+    *sh = Pair<VT>::one(a);
+}
+
+template <int MODE, typename ST, typename VT>
 __global__ void __launch_bounds__(BP_THREADS) k_bp(BpArgs p)
 {
     extern __shared__ float2 bsm[];
@@ -248,12 +355,14 @@ __global__ void __launch_bounds__(BP_THREADS) k_bp(BpArgs p)
         for (int row = warp; row < ns * nc; row += BP_THREADS / 32) {
             const int q = row / nc, t = row - q * nc;
             const int x0 = ws[t];
-            const float* src = p.sino + ((size_t)(ysA + q) * p.T + c0 + t) * p.N;
+            const size_t row_id = (size_t)(ysA + q) * p.T + c0 + t;
+            const ST* src = reinterpret_cast<const ST*>(p.sino) + row_id * p.N;
+            const float sc = std::is_same<ST, float>::value ? 1.f : __ldg(p.scale + row_id);
             float2* dst = pw + q * BP_PSLAB + t * BP_WW;
             for (int k = lane; k < p.ww; k += 32) {
                 const int x = x0 + k;
-                const float a = (x >= 0 && x < p.N) ? __ldg(src + x) : 0.f;
-                const float b = (x + 1 >= 0 && x + 1 < p.N) ? __ldg(src + x + 1) : 0.f;
+                const float a = (x >= 0 && x < p.N) ? Stor<ST>::ld(src + x, sc) : 0.f;
+                const float b = (x + 1 >= 0 && x + 1 < p.N) ? Stor<ST>::ld(src + x + 1, sc) : 0.f;
                 dst[k] = make_float2(a, b);
             }
         }
@@ -339,9 +448,15 @@ __global__ void __launch_bounds__(BP_THREADS) k_bp(BpArgs p)
             for (int i = 0; i < BP_CX; i++) {
                 const int X = X0 + lane + 32 * i;
                 if (Z >= p.GZ || X >= p.GX) continue;
+                float nv[SB];
 #pragma unroll
                 for (int q = 0; q < SB; q++)
-                    if (q < nsl) bp_store<MODE>(p, ys0 + q, Z, X, sum[q][j][i], cnt[j][i]);
+                    nv[q] = q < nsl ? bp_store<MODE>(p, ys0 + q, Z, X, sum[q][j][i], cnt[j][i]) : 0.f;
+                if constexpr (MODE == 0 && !std::is_same<VT, float>::value) {
+#pragma unroll
+                    for (int g = 0; g < SB / 2; g++)
+                        if (2 * g < nsl) shadow_pair<VT>(p, ys0 + 2 * g, Z, X, nv[2 * g], nv[2 * g + 1]);
+                }
             }
         }
         return;
@@ -387,7 +502,10 @@ __global__ void __launch_bounds__(BP_THREADS) k_bp(BpArgs p)
 #pragma unroll
             for (int i = 0; i < BP_CX; i++) {
                 const int X = X0 + lane + 32 * i;
-                if (Z < p.GZ && X < p.GX) bp_store<MODE>(p, ys0 + q, Z, X, sum[j][i], cnt[j][i]);
+                if (Z < p.GZ && X < p.GX) {
+                    const float nv = bp_store<MODE>(p, ys0 + q, Z, X, sum[j][i], cnt[j][i]);
+                    if constexpr (MODE == 0 && !std::is_same<VT, float>::value) shadow_one<VT>(p, ys0 + q, Z, X, nv);
+                }
             }
         }
     }
@@ -466,8 +584,13 @@ __device__ __forceinline__ float bilerp(float a00, float a10, float a01, float a
     return __fmaf_rn(wx, B - A, A);
 }
 
-__global__ void __launch_bounds__(256) k_fp_diff(const float* __restrict__ vol, int Nx, int Nz, int S,
-                                                 const float* __restrict__ raw, float* __restrict__ diff,
+// ST: storage of raw / diff rows; VT: float reads the FP32 volume, __half /
+// __nv_bfloat16 read its 16-bit shadow (two slices per word) — the FP32
+// volume is then read only for slices that may hold "empty" voxels.
+template <typename ST, typename VT>
+__global__ void __launch_bounds__(256) k_fp_diff(const float* __restrict__ vol, const void* __restrict__ shadow,
+                                                 int Nx, int Nz, int S, const ST* __restrict__ raw,
+                                                 ST* __restrict__ diff, const float* __restrict__ scale,
                                                  const float2* __restrict__ cs, int T, int N, int t0,
                                                  double* __restrict__ rf, int* __restrict__ flags)
 {
@@ -490,7 +613,41 @@ __global__ void __launch_bounds__(256) k_fp_diff(const float* __restrict__ vol, 
     float fSum[SB], fCount[SB];
 #pragma unroll
     for (int q = 0; q < SB; q++) { fSum[q] = 0.f; fCount[q] = 0.f; }
-    if (!empty_vox) {
+    bool shadow_done = false;
+    if constexpr (!std::is_same<VT, float>::value) {
+      if (!empty_vox) {
+        shadow_done = true;
+        using T2 = typename Pair<VT>::T2;
+        // two slice pairs; rows of voxel Z and Z + 1 as loop-invariant bases
+        const T2* sbase = reinterpret_cast<const T2*>(shadow) + (size_t)(Nz - 1) * Nx;
+        const T2* r0[SB / 2];
+        const T2* r1[SB / 2];
+#pragma unroll
+        for (int g = 0; g < SB / 2; g++) {
+            r0[g] = sbase + (size_t)((ys0 >> 1) + g) * slice;
+            r1[g] = r0[g] - Nx;
+        }
+        for (int i = wlo; i <= whi; i++) {
+            if (i < lo || i > hi) continue;
+            const float fX = r.x(i), fZ = r.z(i);
+            const int iX = (int)fX, iZ = (int)fZ;
+            const float wx = fX - (float)iX, wz = fZ - (float)iZ;
+            const int o = iX - iZ * Nx;
+#pragma unroll
+            for (int g = 0; g < SB / 2; g++) {
+                const float2 a00 = Pair<VT>::ld(r0[g] + o), a10 = Pair<VT>::ld(r0[g] + o + 1);
+                const float2 a01 = Pair<VT>::ld(r1[g] + o), a11 = Pair<VT>::ld(r1[g] + o + 1);
+                fSum[2 * g] += bilerp(a00.x, a10.x, a01.x, a11.x, wx, wz);
+                fSum[2 * g + 1] += bilerp(a00.y, a10.y, a01.y, a11.y, wx, wz);
+            }
+        }
+        const float n = (float)max(hi - lo + 1, 0);
+#pragma unroll
+        for (int q = 0; q < SB; q++) fCount[q] = n;
+      }
+    }
+    if (shadow_done) {
+    } else if (!empty_vox) {
         // per slice, the rows of voxel Z and Z + 1 as loop-invariant bases; a
         // sample then costs one 32-bit cell offset and one wide add per row
         const float* r0[SB];
@@ -543,8 +700,10 @@ __global__ void __launch_bounds__(256) k_fp_diff(const float* __restrict__ vol, 
         for (int q = 0; q < SB; q++) {
             if (q >= nsl) continue;
             const float fp = fCount[q] <= 0.f ? kSentinelValue : fSum[q] / fCount[q];
-            const size_t o = ((size_t)(ys0 + q) * T + t) * N + u;
-            const float rw = __ldg(raw + o);
+            const size_t row = (size_t)(ys0 + q) * T + t;
+            const size_t o = row * N + u;
+            const float sc = std::is_same<ST, float>::value ? 1.f : __ldg(scale + row);
+            const float rw = Stor<ST>::ld(raw + o, sc);
             float d = 0.f;
             if (!(fp < kSentinelTest) && !(rw < kSentinelTest)) {
                 d = rw - fp;
@@ -552,7 +711,7 @@ __global__ void __launch_bounds__(256) k_fp_diff(const float* __restrict__ vol, 
                 ar += fabsf(rw);
                 if (d <= kLowValue) atomicOr(flags + ys0 + q, kFlagDiffLow);
             }
-            diff[o] = d;
+            Stor<ST>::st(diff + o, d, 1.f / sc);
         }
     }
     if (rf) {

@@ -82,12 +82,16 @@ def units_per_step(c) -> float:
     return float(c["nx"] & ~1) * c["ny"] * c["vol_z"] * len(c["tilts"])
 
 
+STORAGE = {"f32": 0, "f16": 1, "bf16": 2}
+
+
 def plan_kwargs(c) -> dict:
     from aretomo3_b200 import recon
+    st = STORAGE[c.get("storage", "f32")]
     if c["method"] == "sart":
         return dict(method=recon.SART, start_tilt=0, num_tilts=len(c["tilts"]), iterations=c["iters"],
-                    subsets=c["subsets"], relax=c.get("relax", 0.0))
-    return dict(method=recon.WBP)
+                    subsets=c["subsets"], relax=c.get("relax", 0.0), storage=st)
+    return dict(method=recon.WBP, storage=st)
 
 
 # --- clocks -----------------------------------------------------------------
@@ -343,8 +347,9 @@ def run_our_arm(args, c, rank, world, local_rank):
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": c["label"], "name": c["name"], "nx": nx, "ny": ny, "tilts": T, "vol_z": Nz,
+        "vs_baseline": None, "dtype": "f32" if c["storage"] == "f32" else f"{c['storage']}-storage/f32-accumulate",
+        "data": "synthetic",
+        "config": {"workload": c["label"], "name": c["name"], "storage": c["storage"], "nx": nx, "ny": ny, "tilts": T, "vol_z": Nz,
                    "units_per_step": units, "slab_slices": plan.geom.slab_slices or "auto",
                    "l2": "inputs larger than L2 (projections 256 MB, volume 1.26 GB at the default workload)",
                    "parallelism": f"replicas x{world}"},
@@ -373,11 +378,16 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="sart_1k")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--storage", default="f32", choices=sorted(STORAGE),
+                    help="staged-sinogram storage: f32, or f16 / bf16 with per-tilt scale (FP32 accumulation)")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
     local_rank = int(os.environ.get("LOCAL_RANK", 0))
     c = workload(args.workload, seed_offset=rank)
+    c["storage"] = args.storage
+    if args.storage != "f32":
+        c["label"] += f"; {args.storage} storage with per-tilt scale, FP32 accumulation"
     if args.impl == "reference":
         run_reference_arm(args, c, rank, world)
         return

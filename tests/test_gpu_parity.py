@@ -215,3 +215,31 @@ def test_invalid_arguments_raise(R):
         R.Plan(64, 4, np.array([90.0], np.float32), 16)
     with pytest.raises(R.ReconError):
         R.Plan(64, 4, tilts, 16, method=R.SART, iterations=1, subsets=0)
+
+
+PRECISION_TOL = 1e-3   # FP16 / BF16 storage with per-tilt scale, FP32 accumulation
+
+
+@pytest.mark.parametrize("storage", ["f16", "bf16"])
+@pytest.mark.parametrize("mode", ["wbp", "sart"])
+def test_reduced_precision_storage_vs_oracle(R, storage, mode):
+    """Staged sinograms (and, for SART, the residual and the volume the
+    forward projector reads) in 16-bit storage stay within 1e-3 relative L2
+    of the FP64 oracle."""
+    tilts = np.linspace(-60, 60, 41).astype(np.float32)
+    frames = _series(256, 9, tilts, 64, seed=17, noise=2 if mode == "sart" else 1)
+    st = R.STORE_F16 if storage == "f16" else R.STORE_BF16
+    if mode == "wbp":
+        out = ours(R, frames, tilts, dict(mode="wbp", vol_z=64), storage=st)
+        ref = wbp(frames, tilts, 64)
+        f32 = ours(R, frames, tilts, dict(mode="wbp", vol_z=64))
+    else:
+        meta = dict(mode="sart", vol_z=64, start=0, ntilts=41, iters=5, subsets=5)
+        out = ours(R, frames, tilts, meta, storage=st)
+        ref = sart(frames, tilts, 64, 0, 41, 5, 5)
+        f32 = ours(R, frames, tilts, meta)
+    err, err32 = rel_l2(out, ref), rel_l2(f32, ref)
+    print(f"{mode} {storage}: rel-L2 vs FP64 oracle {err:.3e} (FP32 storage {err32:.3e}), "
+          f"max-abs {np.abs(out - ref).max():.3e}")
+    assert np.isfinite(out).all()
+    assert err < PRECISION_TOL
