@@ -36,7 +36,8 @@ def build_at3r(force: bool = False) -> str:
     srcs.append(os.path.join(ROOT, "include", "at3r.h"))
     if force or _newer(out, srcs):
         _run([NVCC, *ARCH, "-O3", "-lineinfo", "-std=c++17", "-shared", "-Xcompiler", "-fPIC",
-              "-I", os.path.join(ROOT, "include"), "-o", out, os.path.join(CSRC, "at3r.cu"), "-ldl"])
+              "-I", os.path.join(ROOT, "include"), "-o", out, os.path.join(CSRC, "at3r.cu"),
+              os.path.join(CSRC, "at3r_server.cpp"), "-ldl", "-lpthread"])
     return out
 
 

@@ -1,6 +1,7 @@
 // C-ABI implementation: plans, workspace, the y-slab loop and the host-buffer
 // path.  Declarations and data layouts: include/at3r.h.
 #include "at3r.h"
+#include "at3r_internal.h"
 #include "recon_kernels.cuh"
 
 #include <cuda_runtime.h>
@@ -90,7 +91,9 @@ void host_fft_pow2(std::vector<std::complex<double>>& a, int sign)
     }
 }
 
-at3r_status make_fft(int n, HostFft& h)
+at3r_status dalloc_bytes(at3r_plan* p, void** ptr, size_t bytes);   // defined with the plan
+
+at3r_status make_fft(at3r_plan* pl, int n, HostFft& h)
 {
     std::vector<int> rad;
     FftPlan& p = h.plan;
@@ -130,7 +133,8 @@ at3r_status make_fft(int n, HostFft& h)
     }
     const size_t cnt = tw.size() + chirp.size() + bhat.size();
     h.bytes = cnt * sizeof(float2);
-    AT3R_CUDA(cudaMalloc(&h.d_tables, h.bytes));
+    at3r_status ra = dalloc_bytes(pl, reinterpret_cast<void**>(&h.d_tables), h.bytes);
+    if (ra != AT3R_OK) return ra;
     std::vector<float2> all;
     all.reserve(cnt);
     all.insert(all.end(), tw.begin(), tw.end());
@@ -216,6 +220,8 @@ struct at3r_plan {
     std::vector<float> tilts;
     int nx = 0, ny = 0, T = 0, N = 0, Nx = 0, Nz = 0, KX = 0;
     int slab = 1;
+    int slab_cap = 1;   // slices the workspace holds; the autotuner picks slab <= slab_cap
+    cudaStream_t alloc_stream = nullptr;   // set: workspace from the memory pool, ordered on this stream
     int device = 0;
     int c2r = AT3R_C2R_HERMITIAN;
     float relax = 1.f;
@@ -258,28 +264,37 @@ struct at3r_plan {
 
 namespace {
 
-template <typename T>
-at3r_status dalloc(at3r_plan* p, T** ptr, size_t count)
+// Workspace allocation: cudaMalloc, or — for plans made by the serving loop —
+// stream-ordered from the device's memory pool on the plan's allocation
+// stream, so that freeing it does not synchronise the device.
+at3r_status dalloc_bytes(at3r_plan* p, void** ptr, size_t bytes)
 {
-    const size_t bytes = count * sizeof(T);
-    cudaError_t e = cudaMalloc((void**)ptr, bytes);
+    cudaError_t e;
+    if (p->alloc_stream) {
+        e = cudaMallocAsync(ptr, bytes, p->alloc_stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(p->alloc_stream);
+    } else {
+        e = cudaMalloc(ptr, bytes);
+    }
     if (e != cudaSuccess) {
         cudaGetLastError();
-        return set_err(AT3R_ERR_OUT_OF_MEMORY, "cudaMalloc of " + std::to_string(bytes) + " bytes failed");
+        return set_err(AT3R_ERR_OUT_OF_MEMORY, "device allocation of " + std::to_string(bytes) + " bytes failed");
     }
     p->ws_bytes += bytes;
     return AT3R_OK;
 }
 
-at3r_status dalloc_bytes(at3r_plan* p, void** ptr, size_t bytes)
+template <typename T>
+at3r_status dalloc(at3r_plan* p, T** ptr, size_t count)
 {
-    cudaError_t e = cudaMalloc(ptr, bytes);
-    if (e != cudaSuccess) {
-        cudaGetLastError();
-        return set_err(AT3R_ERR_OUT_OF_MEMORY, "cudaMalloc of " + std::to_string(bytes) + " bytes failed");
-    }
-    p->ws_bytes += bytes;
-    return AT3R_OK;
+    return dalloc_bytes(p, reinterpret_cast<void**>(ptr), count * sizeof(T));
+}
+
+void dfree(at3r_plan* p, void* ptr)
+{
+    if (!ptr) return;
+    if (p->alloc_stream) cudaFreeAsync(ptr, p->alloc_stream);
+    else cudaFree(ptr);
 }
 
 int bp_window(int tx, int tz, double scale, const std::vector<float>& cs, int T)
@@ -498,7 +513,41 @@ void at3r_geom_init(at3r_geom* g, int method)
     g->c2r = AT3R_C2R_MATCH_CUFFT;
 }
 
-at3r_status at3r_plan_create(const at3r_geom* g, at3r_plan** out)
+at3r_status plan_create_impl(const at3r_geom* g, cudaStream_t alloc_stream, at3r_plan** out);
+
+at3r_status at3r_plan_create(const at3r_geom* g, at3r_plan** out) { return plan_create_impl(g, nullptr, out); }
+
+// Device bytes a plan and one at3r_run_host over it hold (workspace, FFT
+// tables, the host path's two slab buffers), without allocating; an upper
+// estimate the serving loop admits requests by.
+size_t at3r_plan_estimate_bytes(const at3r_geom* g)
+{
+    if (!g || g->nx < 1 || g->ny < 1 || g->n_tilts < 1 || g->vol_z < 1) return 0;
+    const size_t T = g->n_tilts, N = g->nx & ~1, Nx = N, Nz = g->vol_z, KX = Nx / 2 + 1, nx = g->nx;
+    const size_t esz = g->storage == AT3R_STORE_F32 ? 4 : 2;
+    size_t per_slice, tables = 0;
+    if (g->method == AT3R_SART) {
+        per_slice = 2 * T * N * sizeof(float) + Nx * Nz * sizeof(float);
+    } else {
+        per_slice = T * N * sizeof(float) + 16 * Nx * Nz + 2 * Nz * KX * sizeof(float2);
+        tables = 4 * sizeof(float2) * 4 * (N + 2 * Nx + 3 * Nz + Nx);   // Bluestein can take 4x the length
+    }
+    size_t slab = g->slab_slices;
+    if (slab <= 0) {
+        const size_t budget = g->method == AT3R_SART ? ((size_t)96 << 20) : ((size_t)256 << 20);
+        slab = std::max<size_t>(8, std::max<size_t>(1, budget / per_slice));
+    }
+    slab = std::min<size_t>(slab, (size_t)g->ny);
+    size_t work;
+    if (g->method == AT3R_SART)
+        work = slab * (2 * T * N * esz + (esz < 4 ? 2 * Nx * Nz + T * 4 : 0)) + slab * 8;
+    else
+        work = slab * (T * N * esz + 16 * Nx * Nz + 2 * Nz * KX * sizeof(float2) + (esz < 4 ? T * 4 : 0) + 4);
+    const size_t host_path = 2 * (T * slab * nx + slab * Nx * Nz) * sizeof(float);
+    return work + host_path + tables + T * 8 + (1 << 20);
+}
+
+at3r_status plan_create_impl(const at3r_geom* g, cudaStream_t alloc_stream, at3r_plan** out)
 {
     if (!g || !out) return set_err(AT3R_ERR_INVALID_ARGUMENT, "null argument");
     *out = nullptr;
@@ -522,6 +571,7 @@ at3r_status at3r_plan_create(const at3r_geom* g, at3r_plan** out)
         return set_err(AT3R_ERR_NO_DEVICE, "no CUDA device");
     }
     at3r_plan* p = new at3r_plan();
+    p->alloc_stream = alloc_stream;
     p->g = *g;
     p->esz = g->storage == AT3R_STORE_F32 ? sizeof(float) : 2;
     p->tilts.assign(g->tilts_deg, g->tilts_deg + g->n_tilts);
@@ -567,11 +617,11 @@ at3r_status at3r_plan_create(const at3r_geom* g, at3r_plan** out)
         per_slice = 2 * T * N * sizeof(float) + Nx * Nz * sizeof(float);
     } else {
         p->c2r = g->c2r == AT3R_C2R_MATCH_CUFFT ? probe_cufft_c2r(p->Nz, p->Nx) : g->c2r;
-        if ((rc = make_fft(p->N, p->fN))) return fail(rc);
-        if ((rc = make_fft(2 * p->Nx, p->f2x))) return fail(rc);
-        if ((rc = make_fft(2 * p->Nz, p->f2z))) return fail(rc);
-        if ((rc = make_fft(p->Nz, p->fz))) return fail(rc);
-        if ((rc = make_fft(p->Nx, p->fx))) return fail(rc);
+        if ((rc = make_fft(p, p->N, p->fN))) return fail(rc);
+        if ((rc = make_fft(p, 2 * p->Nx, p->f2x))) return fail(rc);
+        if ((rc = make_fft(p, 2 * p->Nz, p->f2z))) return fail(rc);
+        if ((rc = make_fft(p, p->Nz, p->fz))) return fail(rc);
+        if ((rc = make_fft(p, p->Nx, p->fx))) return fail(rc);
         p->smem_rweight = 2 * sizeof(float2) * p->fN.plan.work;
         p->smem_row = 2 * sizeof(float2) * p->f2x.plan.work;
         p->smem_xc2r = 2 * sizeof(float2) * p->fx.plan.work;
@@ -610,6 +660,7 @@ at3r_status at3r_plan_create(const at3r_geom* g, at3r_plan** out)
         slab = std::max(slab, 8);
     }
     p->slab = std::min(slab, p->ny);
+    p->slab_cap = p->slab;
     const size_t S = p->slab;
     if (g->method == AT3R_SART) {
         if ((rc = dalloc_bytes(p, &p->d_raw, S * T * N * p->esz))) return fail(rc);
@@ -636,10 +687,12 @@ at3r_status at3r_plan_create(const at3r_geom* g, at3r_plan** out)
 void at3r_plan_destroy(at3r_plan* p)
 {
     if (!p) return;
-    cudaFree(p->d_cs); cudaFree(p->d_raw); cudaFree(p->d_diff); cudaFree(p->d_scale); cudaFree(p->d_shadow); cudaFree(p->d_flags); cudaFree(p->d_rf);
-    cudaFree(p->d_h); cudaFree(p->d_filt); cudaFree(p->d_g2); cudaFree(p->d_y);
-    for (HostFft* f : {&p->fN, &p->f2x, &p->f2z, &p->fz, &p->fx}) cudaFree(f->d_tables);
-    for (int i = 0; i < 2; i++) { cudaFree(p->d_proj_slab[i]); cudaFree(p->d_vol_slab[i]); }
+    for (void* ptr : {(void*)p->d_cs, (void*)p->d_raw, (void*)p->d_diff, (void*)p->d_scale, (void*)p->d_shadow,
+                      (void*)p->d_flags, (void*)p->d_rf, (void*)p->d_h, (void*)p->d_filt, (void*)p->d_g2,
+                      (void*)p->d_y})
+        dfree(p, ptr);
+    for (HostFft* f : {&p->fN, &p->f2x, &p->f2z, &p->fz, &p->fx}) dfree(p, f->d_tables);
+    for (int i = 0; i < 2; i++) { dfree(p, p->d_proj_slab[i]); dfree(p, p->d_vol_slab[i]); }
     if (p->s_copy_in) cudaStreamDestroy(p->s_copy_in);
     if (p->s_copy_out) cudaStreamDestroy(p->s_copy_out);
     for (cudaEvent_t& e : p->ev) if (e) cudaEventDestroy(e);
@@ -775,6 +828,12 @@ const char* at3r_status_str(at3r_status s)
 }
 
 const char* at3r_last_error(void) { return g_last_error.c_str(); }
+
+}  // extern "C"
+
+void at3r_set_last_error(const char* msg) { g_last_error = msg ? msg : ""; }
+
+extern "C" {
 
 }  // extern "C"
 
@@ -920,3 +979,155 @@ extern "C" at3r_status at3r_sart_device_noalloc(const float* proj, int nx, int n
     }
     return AT3R_OK;
 }
+
+// ===========================================================================
+// Batched form: many series in one CUDA graph, and the slab autotuner.
+// ===========================================================================
+struct at3r_batch {
+    std::vector<at3r_plan*> plans;
+    std::vector<const float*> proj;
+    std::vector<float*> vol;
+    int branches = 1;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    std::vector<cudaStream_t> streams;
+    std::vector<cudaEvent_t> events;
+};
+
+namespace {
+
+// Slab sizes the autotuner tries (slices per device batch, up to the plan's
+// workspace capacity) and the best one found per problem shape.
+std::mutex g_tune_mu;
+std::map<std::vector<int>, int> g_tune_cache;
+
+std::vector<int> tune_key(const at3r_plan* p)
+{
+    return {p->g.method, p->nx, p->Nz, p->T, p->g.storage, p->g.iterations, (int)p->sub_size.size(), p->slab_cap};
+}
+
+}  // namespace
+
+extern "C" {
+
+at3r_status at3r_plan_autotune(at3r_plan* p, const float* proj, float* vol, void* stream, int* chosen)
+{
+    if (!p || !proj || !vol) return set_err(AT3R_ERR_INVALID_ARGUMENT, "null argument");
+    const auto key = tune_key(p);
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        auto it = g_tune_cache.find(key);
+        if (it != g_tune_cache.end()) {
+            p->slab = it->second;
+            if (chosen) *chosen = p->slab;
+            return AT3R_OK;
+        }
+    }
+    cudaStream_t st = (cudaStream_t)stream;
+    std::vector<int> cand;
+    for (int s = SB; s < p->slab_cap; s *= 2) cand.push_back(s);
+    cand.push_back(p->slab_cap);
+    cudaEvent_t e0, e1;
+    AT3R_CUDA(cudaEventCreate(&e0));
+    AT3R_CUDA(cudaEventCreate(&e1));
+    const bool timing = p->timing;
+    p->timing = false;
+    int best = p->slab_cap;
+    float best_ms = 3.0e38f;
+    at3r_status rc = AT3R_OK;
+    for (int s : cand) {
+        p->slab = s;
+        if ((rc = at3r_run_device(p, proj, vol, stream))) break;   // warm-up
+        cudaEventRecord(e0, st);
+        if ((rc = at3r_run_device(p, proj, vol, stream))) break;
+        cudaEventRecord(e1, st);
+        cudaEventSynchronize(e1);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (ms < best_ms) { best_ms = ms; best = s; }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    p->timing = timing;
+    p->slab = best;
+    if (rc) return rc;
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_tune_cache[key] = best;
+    if (chosen) *chosen = best;
+    return AT3R_OK;
+}
+
+at3r_status at3r_batch_create(at3r_plan* const* plans, const float* const* proj, float* const* vol, int n,
+                              int branches, at3r_batch** out)
+{
+    if (!plans || !proj || !vol || !out || n < 1) return set_err(AT3R_ERR_INVALID_ARGUMENT, "null argument or n < 1");
+    for (int i = 0; i < n; i++) {
+        if (!plans[i] || !proj[i] || !vol[i]) return set_err(AT3R_ERR_INVALID_ARGUMENT, "null plan or buffer");
+        if (plans[i]->g.method == AT3R_SART && plans[i]->g.compute_rfactor)
+            return set_err(AT3R_ERR_UNSUPPORTED, "a batched SART plan cannot copy its R-factor to the host");
+        if (plans[i]->timing) return set_err(AT3R_ERR_UNSUPPORTED, "disable per-kernel timing on batched plans");
+    }
+    at3r_batch* b = new at3r_batch();
+    b->plans.assign(plans, plans + n);
+    b->proj.assign(proj, proj + n);
+    b->vol.assign(vol, vol + n);
+    b->branches = std::max(1, std::min(branches, n));
+    *out = b;
+    return AT3R_OK;
+}
+
+// Captures (on first use) every plan's launches into one graph — plan i on
+// branch i % branches, forked from and joined back to `stream` — and then
+// replays the whole batch as one graph launch.
+at3r_status at3r_batch_run(at3r_batch* b, void* stream)
+{
+    if (!b) return set_err(AT3R_ERR_INVALID_ARGUMENT, "null batch");
+    cudaStream_t st = (cudaStream_t)stream;
+    if (!b->exec) {
+        cudaStream_t cap = nullptr;
+        AT3R_CUDA(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
+        b->streams.assign(b->branches, nullptr);
+        b->events.assign(b->branches + 1, nullptr);
+        for (auto& s2 : b->streams) AT3R_CUDA(cudaStreamCreateWithFlags(&s2, cudaStreamNonBlocking));
+        for (auto& e : b->events) AT3R_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        AT3R_CUDA(cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal));
+        at3r_status rc = AT3R_OK;
+        AT3R_CUDA(cudaEventRecord(b->events[0], cap));
+        for (int k = 0; k < b->branches && !rc; k++)
+            if (cudaStreamWaitEvent(b->streams[k], b->events[0], 0) != cudaSuccess) rc = AT3R_ERR_CUDA;
+        for (size_t i = 0; i < b->plans.size() && !rc; i++)
+            rc = at3r_run_device(b->plans[i], b->proj[i], b->vol[i], b->streams[i % b->branches]);
+        for (int k = 0; k < b->branches && !rc; k++) {
+            if (cudaEventRecord(b->events[k + 1], b->streams[k]) != cudaSuccess ||
+                cudaStreamWaitEvent(cap, b->events[k + 1], 0) != cudaSuccess)
+                rc = AT3R_ERR_CUDA;
+        }
+        cudaGraph_t g = nullptr;
+        const cudaError_t ce = cudaStreamEndCapture(cap, &g);
+        cudaStreamDestroy(cap);
+        if (rc || ce != cudaSuccess) {
+            if (g) cudaGraphDestroy(g);
+            cudaGetLastError();
+            return set_err(AT3R_ERR_CUDA, std::string("batch capture failed: ") +
+                                              (rc ? at3r_last_error() : cudaGetErrorString(ce)));
+        }
+        b->graph = g;
+        AT3R_CUDA(cudaGraphInstantiate(&b->exec, b->graph, 0));
+    }
+    AT3R_CUDA(cudaGraphLaunch(b->exec, st));
+    return AT3R_OK;
+}
+
+void at3r_batch_destroy(at3r_batch* b)
+{
+    if (!b) return;
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    if (b->graph) cudaGraphDestroy(b->graph);
+    for (auto s2 : b->streams) if (s2) cudaStreamDestroy(s2);
+    for (auto e : b->events) if (e) cudaEventDestroy(e);
+    delete b;
+}
+
+int at3r_plan_slab(const at3r_plan* p) { return p ? p->slab : 0; }
+
+}  // extern "C"

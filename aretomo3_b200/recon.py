@@ -62,6 +62,22 @@ _EXPORTS = {
     "at3r_plan_kernel_stats": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_char_p),
                                               ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_double),
                                               ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]),
+    "at3r_plan_autotune": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                          ctypes.POINTER(ctypes.c_int)]),
+    "at3r_plan_slab": (ctypes.c_int, [ctypes.c_void_p]),
+    "at3r_batch_create": (ctypes.c_int, [ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_void_p),
+                                         ctypes.POINTER(ctypes.c_void_p), ctypes.c_int, ctypes.c_int,
+                                         ctypes.POINTER(ctypes.c_void_p)]),
+    "at3r_batch_run": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
+    "at3r_batch_destroy": (None, [ctypes.c_void_p]),
+    "at3r_plan_estimate_bytes": (ctypes.c_size_t, [ctypes.POINTER(Geom)]),
+    "at3r_server_create": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)]),
+    "at3r_server_submit": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(Geom), ctypes.POINTER(ctypes.c_void_p),
+                                          ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_int64)]),
+    "at3r_server_wait": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int64, ctypes.POINTER(ctypes.c_double),
+                                        ctypes.POINTER(ctypes.c_double)]),
+    "at3r_server_in_use_bytes": (ctypes.c_size_t, [ctypes.c_void_p]),
+    "at3r_server_destroy": (None, [ctypes.c_void_p]),
     "at3r_status_str": (ctypes.c_char_p, [ctypes.c_int]),
     "at3r_last_error": (ctypes.c_char_p, []),
 }
@@ -84,6 +100,24 @@ def _check(rc: int) -> None:
         raise ReconError(rc, f"{L.at3r_status_str(rc).decode()}: {L.at3r_last_error().decode()}")
 
 
+def make_geom(nx, ny, tilts_deg, vol_z, method=WBP, start_tilt=0, num_tilts=None, iterations=0, subsets=1,
+              relax=0.0, storage=STORE_F32, c2r=C2R_MATCH_CUFFT, slab_slices=0, compute_rfactor=False):
+    """Fills an at3r_geom; returns it with the tilt array it points into
+    (which the caller keeps alive as long as the struct)."""
+    tilts = np.ascontiguousarray(np.asarray(tilts_deg, dtype=np.float32))
+    g = Geom()
+    lib().at3r_geom_init(ctypes.byref(g), method)
+    g.nx, g.ny, g.n_tilts = int(nx), int(ny), int(tilts.size)
+    g.tilts_deg = tilts.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+    g.vol_z = int(vol_z)
+    g.start_tilt = int(start_tilt)
+    g.num_tilts = int(tilts.size if num_tilts is None else num_tilts)
+    g.iterations, g.subsets, g.relax = int(iterations), int(subsets), float(relax)
+    g.storage, g.c2r, g.slab_slices = int(storage), int(c2r), int(slab_slices)
+    g.compute_rfactor = int(bool(compute_rfactor))
+    return g, tilts
+
+
 class Plan:
     """One reconstruction plan (geometry, parameters and device workspace)."""
 
@@ -91,17 +125,8 @@ class Plan:
                  subsets=1, relax=0.0, storage=STORE_F32, c2r=C2R_MATCH_CUFFT, slab_slices=0,
                  compute_rfactor=False):
         L = lib()
-        self._tilts = np.ascontiguousarray(np.asarray(tilts_deg, dtype=np.float32))
-        g = Geom()
-        L.at3r_geom_init(ctypes.byref(g), method)
-        g.nx, g.ny, g.n_tilts = int(nx), int(ny), int(self._tilts.size)
-        g.tilts_deg = self._tilts.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
-        g.vol_z = int(vol_z)
-        g.start_tilt = int(start_tilt)
-        g.num_tilts = int(self._tilts.size if num_tilts is None else num_tilts)
-        g.iterations, g.subsets, g.relax = int(iterations), int(subsets), float(relax)
-        g.storage, g.c2r, g.slab_slices = int(storage), int(c2r), int(slab_slices)
-        g.compute_rfactor = int(bool(compute_rfactor))
+        g, self._tilts = make_geom(nx, ny, tilts_deg, vol_z, method, start_tilt, num_tilts, iterations, subsets,
+                                   relax, storage, c2r, slab_slices, compute_rfactor)
         self.geom = g
         self.method = method
         self.iterations = int(iterations)
@@ -157,6 +182,18 @@ class Plan:
     def c2r(self) -> int:
         return int(lib().at3r_plan_c2r(self._h))
 
+    def autotune(self, proj_ptr: int, vol_ptr: int, stream: int = 0) -> int:
+        """Times candidate slab sizes on the given device buffers (overwritten)
+        and keeps the fastest; returns it."""
+        chosen = ctypes.c_int()
+        _check(lib().at3r_plan_autotune(self._h, ctypes.c_void_p(proj_ptr), ctypes.c_void_p(vol_ptr),
+                                        ctypes.c_void_p(stream), ctypes.byref(chosen)))
+        return chosen.value
+
+    @property
+    def slab(self) -> int:
+        return int(lib().at3r_plan_slab(self._h))
+
     def set_timing(self, enable: bool) -> None:
         _check(lib().at3r_plan_set_timing(self._h, int(bool(enable))))
 
@@ -175,6 +212,98 @@ class Plan:
             if la.value:
                 out[name.value.decode()] = dict(launches=la.value, ms=ms.value, bytes=by.value, units=un.value)
         return out
+
+
+class Batch:
+    """Several plans over device-resident series, captured into one CUDA graph
+    (independent series on parallel branches) and replayed as one launch."""
+
+    def __init__(self, plans, proj_ptrs, vol_ptrs, branches: int = 4):
+        n = len(plans)
+        P = ctypes.c_void_p * n
+        self._plans = list(plans)   # keep the plans alive
+        h = ctypes.c_void_p()
+        _check(lib().at3r_batch_create(P(*[p._h.value for p in plans]), P(*proj_ptrs), P(*vol_ptrs), n,
+                                       int(branches), ctypes.byref(h)))
+        self._h = h
+
+    def run(self, stream: int = 0) -> None:
+        _check(lib().at3r_batch_run(self._h, ctypes.c_void_p(stream)))
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().at3r_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def estimate_bytes(nx, ny, tilts_deg, vol_z, **kw) -> int:
+    """Device bytes a plan plus one host-path run hold, by estimate (no GPU)."""
+    g, _t = make_geom(nx, ny, tilts_deg, vol_z, **kw)
+    return int(lib().at3r_plan_estimate_bytes(ctypes.byref(g)))
+
+
+class ServerOpts(ctypes.Structure):
+    _fields_ = [("hbm_budget_bytes", ctypes.c_size_t), ("max_inflight", ctypes.c_int)]
+
+
+class Server:
+    """Serving loop on the current device (at3r_server_*): tilt series are
+    submitted as they arrive and reconstructed concurrently, admitted in FIFO
+    order against an HBM budget and a number of in-flight slots."""
+
+    def __init__(self, hbm_budget_bytes: int = 0, max_inflight: int = 4):
+        o = ServerOpts(int(hbm_budget_bytes), int(max_inflight))
+        h = ctypes.c_void_p()
+        _check(lib().at3r_server_create(ctypes.byref(o), ctypes.byref(h)))
+        self._h = h
+        self._keep = {}
+
+    def submit(self, frames: np.ndarray, tilts_deg, vol_z: int, out: np.ndarray | None = None, **kw) -> int:
+        """frames: host float32 [T][ny][nx] (pinned memory overlaps best);
+        returns a request id.  The volume lands in `out` (allocated if None),
+        which wait() returns."""
+        frames = np.ascontiguousarray(frames, dtype=np.float32)
+        T, ny, nx = frames.shape
+        g, tilts = make_geom(nx, ny, tilts_deg, vol_z, **kw)
+        if out is None:
+            out = np.empty((ny, int(vol_z), nx & ~1), np.float32)
+        fin = (ctypes.c_void_p * T)(*[frames[t].ctypes.data for t in range(T)])
+        fout = (ctypes.c_void_p * ny)(*[out[y].ctypes.data for y in range(ny)])
+        rid = ctypes.c_int64()
+        _check(lib().at3r_server_submit(self._h, ctypes.byref(g), fin, fout, ctypes.byref(rid)))
+        self._keep[rid.value] = (frames, out, tilts, fin, fout)
+        return rid.value
+
+    def wait(self, rid: int):
+        """Blocks until the request is done; returns (volume, latency_s, queued_s)."""
+        lat, q = ctypes.c_double(), ctypes.c_double()
+        try:
+            _check(lib().at3r_server_wait(self._h, int(rid), ctypes.byref(lat), ctypes.byref(q)))
+        finally:
+            kept = self._keep.pop(int(rid), None)
+        return kept[1], lat.value, q.value
+
+    @property
+    def in_use_bytes(self) -> int:
+        return int(lib().at3r_server_in_use_bytes(self._h))
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().at3r_server_destroy(self._h)
+            self._h = None
+            self._keep.clear()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 # --- reference-shaped entry points -----------------------------------------

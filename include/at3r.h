@@ -136,6 +136,56 @@ at3r_status at3r_sart_device_noalloc(const float* proj, int nx, int ny, int n_ti
                                      int vol_z, int start_tilt, int num_tilts, int iterations, int subsets,
                                      float relax, float* vol, void* stream);
 
+/* Slab autotuner: times at3r_run_device with slab sizes from 4 slices up to
+ * the plan's workspace capacity (doubling) on proj / vol (device buffers in
+ * the layouts above, overwritten) and keeps the fastest for the plan.  The
+ * choice is cached per problem shape, so later plans of the same shape skip
+ * the timing.  *chosen (may be NULL) receives the slab. */
+at3r_status at3r_plan_autotune(at3r_plan* plan, const float* proj, float* vol, void* stream, int* chosen);
+/* Slices per device batch the plan currently uses. */
+int at3r_plan_slab(const at3r_plan* plan);
+
+/* Batched form: a fixed set of plans over device-resident series.  The first
+ * at3r_batch_run captures every plan's launches into one CUDA graph (plan i
+ * on branch i % branches, so independent series overlap on the device) and
+ * every run replays it as a single graph launch on `stream`.  Plans, buffers
+ * and their contents' sizes must stay as given; SART plans must not compute
+ * the R-factor and no plan may have timing enabled. */
+typedef struct at3r_batch at3r_batch;
+at3r_status at3r_batch_create(at3r_plan* const* plans, const float* const* proj, float* const* vol, int n,
+                              int branches, at3r_batch** out);
+at3r_status at3r_batch_run(at3r_batch* batch, void* stream);
+void at3r_batch_destroy(at3r_batch* batch);
+
+/* Upper estimate of the device bytes that at3r_plan_create plus one
+ * at3r_run_host over the plan hold (workspace, FFT tables, the two slab
+ * buffers of the host path); no device needed.  0 for invalid sizes. */
+size_t at3r_plan_estimate_bytes(const at3r_geom* g);
+
+/* Serving loop (on the current device).  Series are submitted as they are
+ * collected and reconstructed concurrently: a request waits in FIFO order
+ * until the device bytes it needs fit hbm_budget_bytes beside the running
+ * ones and one of max_inflight workers (each with its own stream) is free;
+ * its volume streams back slab by slab.  Frames and volume frames are host
+ * buffers as for at3r_run_host (pinned memory overlaps best) and must stay
+ * valid until at3r_server_wait returns for the request.  Results equal those
+ * of a lone at3r_run_host on the same geometry. */
+typedef struct at3r_server at3r_server;
+typedef struct at3r_server_opts {
+    size_t hbm_budget_bytes;   /* 0 = 90% of the device memory free at creation */
+    int max_inflight;          /* 0 = 4 */
+} at3r_server_opts;
+at3r_status at3r_server_create(const at3r_server_opts* opts, at3r_server** out);
+at3r_status at3r_server_submit(at3r_server* server, const at3r_geom* g, const float* const* frames,
+                               float* const* vol_frames, int64_t* id);
+/* Blocks until request `id` is done; its status; latency from submission to
+ * the volume in host memory, and the part of it spent queued. */
+at3r_status at3r_server_wait(at3r_server* server, int64_t id, double* latency_s, double* queued_s);
+/* Device bytes currently admitted (by estimate). */
+size_t at3r_server_in_use_bytes(at3r_server* server);
+/* Waits for every submitted request, then releases the workers. */
+void at3r_server_destroy(at3r_server* server);
+
 const char* at3r_status_str(at3r_status s);
 const char* at3r_last_error(void);
 

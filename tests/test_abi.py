@@ -62,3 +62,15 @@ def test_valid_geometry_without_gpu_reports_no_device():
     with pytest.raises(recon.ReconError) as ei:
         recon.Plan(64, 4, np.linspace(-60, 60, 11), 16)
     assert ei.value.status == 6  # AT3R_ERR_NO_DEVICE
+
+
+def test_estimate_bytes_without_gpu():
+    from aretomo3_b200 import recon
+    tilts = np.linspace(-60, 60, 41)
+    small = recon.estimate_bytes(256, 64, tilts, 64)
+    assert small > 0
+    assert recon.estimate_bytes(512, 64, tilts, 128) > small
+    # a 4k series holds at least its two host-path slab buffers and the slab workspace
+    big = recon.estimate_bytes(4096, 4096, tilts, 1200, method=recon.SART, storage=recon.STORE_F16)
+    assert big > 2 * 8 * 4096 * 1200 * 4
+    assert recon.estimate_bytes(0, 64, tilts, 64) == 0
