@@ -1035,11 +1035,24 @@ at3r_status at3r_plan_autotune(at3r_plan* p, const float* proj, float* vol, void
     int best = p->slab_cap;
     float best_ms = 3.0e38f;
     at3r_status rc = AT3R_OK;
+    // every candidate is timed on the same leading rows (slab cost is the
+    // same along y), at most two of the largest slabs
+    const int rows = std::min(p->ny, 2 * p->slab_cap);
+    const size_t tilt_stride = (size_t)p->ny * p->nx;
+    auto run_rows = [&]() -> at3r_status {
+        at3r_status r;
+        if ((r = begin_run(p, st))) return r;
+        for (int y0 = 0; y0 < rows; y0 += p->slab) {
+            const int S = std::min(p->slab, rows - y0);
+            if ((r = run_slab(p, proj, tilt_stride, y0, S, vol + (size_t)y0 * p->Nx * p->Nz, st))) return r;
+        }
+        return end_run(p, st);
+    };
     for (int s : cand) {
         p->slab = s;
-        if ((rc = at3r_run_device(p, proj, vol, stream))) break;   // warm-up
+        if ((rc = run_rows())) break;   // warm-up
         cudaEventRecord(e0, st);
-        if ((rc = at3r_run_device(p, proj, vol, stream))) break;
+        if ((rc = run_rows())) break;
         cudaEventRecord(e1, st);
         cudaEventSynchronize(e1);
         float ms = 0.f;

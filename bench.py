@@ -370,6 +370,252 @@ def run_our_arm(args, c, rank, world, local_rank):
     plan.close()
 
 
+# --- batched form: many uneven series in one graph launch --------------------
+def batch_specs(n, seed=7):
+    """Uneven series: nx, ny in {512..2048 step 256}, 31..61 tilts over +-60
+    degrees, thickness 128..600."""
+    from aretomo3_b200 import synth
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(n):
+        nx = 512 + 256 * int(rng.integers(0, 7))
+        ny = 512 + 256 * int(rng.integers(0, 7))
+        nt = int(rng.integers(31, 62))
+        vz = int(rng.integers(128, 601))
+        ph = synth.Phantom(seed=500 + i, n_ellipsoids=200, n_beads=20)
+        out.append(dict(nx=nx, ny=ny, tilts=np.linspace(-60, 60, nt).astype(np.float32), vol_z=vz, phantom=ph))
+    return out
+
+
+def run_batch_arm(args):
+    import torch
+    from aretomo3_b200 import recon, synth
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    stream = torch.cuda.current_stream(dev)
+    specs = batch_specs(args.series)
+    st = STORAGE[args.storage]
+    clocks = ClockSampler(0)
+    clocks.start()
+    tot_units, ms_graph, ms_plain, equal, slabs, launches = 0.0, 0.0, 0.0, True, [], 0
+    for g0 in range(0, len(specs), args.group):
+        grp = specs[g0:g0 + args.group]
+        projs, vols, plans = [], [], []
+        for c in grp:
+            fr = synth.make_tilt_series(c["nx"], c["ny"], c["tilts"], c["vol_z"], c["phantom"])
+            projs.append(torch.from_numpy(fr).to(dev))
+            pl = recon.Plan(c["nx"], c["ny"], c["tilts"], c["vol_z"], method=recon.WBP, storage=st)
+            vols.append(torch.empty(pl.volume_shape, device=dev, dtype=torch.float32))
+            plans.append(pl)
+            tot_units += units_per_step(c)
+        for pl, pj, v in zip(plans, projs, vols):
+            slabs.append(pl.autotune(pj.data_ptr(), v.data_ptr(), stream.cuda_stream))
+        # plain: per-series launches, one after another on one stream
+        for _ in range(args.warmup):
+            for pl, pj, v in zip(plans, projs, vols):
+                pl.run_device(pj.data_ptr(), v.data_ptr(), stream.cuda_stream)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            for pl, pj, v in zip(plans, projs, vols):
+                pl.run_device(pj.data_ptr(), v.data_ptr(), stream.cuda_stream)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms_plain += e0.elapsed_time(e1)
+        launches += sum(pl.last_launches for pl in plans) * args.steps
+        ref = [v.clone() for v in vols]
+        batch = recon.Batch(plans, [p.data_ptr() for p in projs], [v.data_ptr() for v in vols],
+                            branches=args.branches)
+        for v in vols:
+            v.fill_(float("nan"))
+        for _ in range(args.warmup):   # the first run captures the graph
+            batch.run(stream.cuda_stream)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(args.steps):
+            batch.run(stream.cuda_stream)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms_graph += e0.elapsed_time(e1)
+        equal = equal and all(torch.equal(a, b) for a, b in zip(vols, ref))
+        batch.close()
+        for pl in plans:
+            pl.close()
+        del projs, vols, ref
+        torch.cuda.empty_cache()
+    clk = clocks.stop()
+    value = tot_units * args.steps / (ms_graph / 1e3) / 1e9
+    plain = tot_units * args.steps / (ms_plain / 1e3) / 1e9
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms_graph / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32" if args.storage == "f32" else f"{args.storage}-storage/f32-accumulate",
+            "data": "synthetic",
+            "config": {"workload": f"batched WBP: {len(specs)} seeded series, nx, ny in 512..2048 step 256, "
+                                   f"31..61 tilts over +-60 deg, thickness 128..600; groups of {args.group} "
+                                   f"resident series, each group one CUDA-graph launch on {args.branches} branches",
+                       "name": "batch_uneven", "storage": args.storage, "series": len(specs),
+                       "units_per_step": tot_units,
+                       "l2": "inputs larger than L2 (each group holds tens of GB of series and volumes)"},
+            "plain_launches": {"value": plain, "unit": UNIT, "ms_per_step": ms_plain / args.steps},
+            "speedup_vs_plain": value / plain, "graph_equals_plain": bool(equal),
+            "autotuned_slabs": {str(k): slabs.count(k) for k in sorted(set(slabs))},
+            "gpu_launches": int(launches), "clocks": clk}
+    print(json.dumps(line), flush=True)
+
+
+# --- serving form: Poisson arrivals through the request loop ------------------
+def serve_pool(n, seed=11):
+    """Distinct seeded series the requests draw from: nx, ny in {256..1024
+    step 128}, 31..61 tilts over +-60 degrees, thickness 64..300."""
+    from aretomo3_b200 import synth
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(n):
+        nx = 128 * int(rng.integers(2, 9))
+        ny = 128 * int(rng.integers(2, 9))
+        nt = int(rng.integers(31, 62))
+        vz = int(rng.integers(64, 301))
+        ph = synth.Phantom(seed=900 + i, n_ellipsoids=150, n_beads=15)
+        out.append(dict(nx=nx, ny=ny, tilts=np.linspace(-60, 60, nt).astype(np.float32), vol_z=vz, phantom=ph))
+    return out
+
+
+def serve_once(pool, frames, reqs, arrivals, storage, inflight, budget, out_bufs):
+    """Feeds the requests to a server at their arrival times; returns per
+    request (latency from arrival, queued) and the makespan."""
+    import threading as th
+    from aretomo3_b200 import recon
+    srv = recon.Server(hbm_budget_bytes=budget, max_inflight=inflight)
+    free = list(range(len(out_bufs)))
+    cv = th.Condition()
+    order = []   # (id, request index, buffer, submit time)
+    lat = [None] * len(reqs)
+    done_evt = th.Event()
+
+    def waiter():
+        k = 0
+        while k < len(reqs):
+            with cv:
+                while k >= len(order):
+                    cv.wait()
+                rid, i, b, t_sub = order[k]
+            _, l, q = srv.wait(rid)
+            lat[i] = (t_sub - t0 - arrivals[i] + l, q)
+            with cv:
+                free.append(b)
+                cv.notify_all()
+            k += 1
+        done_evt.set()
+
+    w = th.Thread(target=waiter, daemon=True)
+    t0 = time.perf_counter()
+    w.start()
+    for i, (pi, sart) in enumerate(reqs):
+        c = pool[pi]
+        delay = t0 + arrivals[i] - time.perf_counter()
+        if delay > 0:
+            time.sleep(delay)
+        with cv:
+            while not free:
+                cv.wait()
+            b = free.pop()
+        Nx = c["nx"] & ~1
+        out = out_bufs[b][: c["ny"] * c["vol_z"] * Nx].reshape(c["ny"], c["vol_z"], Nx)
+        kw = dict(method=1, iterations=10, subsets=5) if sart else dict(method=0)
+        rid = srv.submit(frames[pi], c["tilts"], c["vol_z"], out=out, storage=storage, **kw)
+        with cv:
+            order.append((rid, i, b, time.perf_counter()))
+            cv.notify_all()
+    done_evt.wait()
+    makespan = time.perf_counter() - t0
+    srv.close()
+    return lat, makespan
+
+
+def run_serving_arm(args):
+    import torch
+    from aretomo3_b200 import recon, synth
+    torch.cuda.set_device(0)
+    pool = serve_pool(args.pool)
+    frames = [torch.from_numpy(synth.make_tilt_series(c["nx"], c["ny"], c["tilts"], c["vol_z"], c["phantom"]))
+              .pin_memory().numpy() for c in pool]
+    rng = np.random.default_rng(12)
+    n = args.requests
+    reqs = [(int(rng.integers(0, len(pool))), bool(rng.random() < 0.3)) for _ in range(n)]
+    arrivals = np.cumsum(rng.exponential(args.interarrival, n))
+    arrivals -= arrivals[0]
+    vmax = max(c["ny"] * c["vol_z"] * (c["nx"] & ~1) for c in pool)
+    out_bufs = [torch.empty(vmax, dtype=torch.float32).pin_memory().numpy() for _ in range(args.out_buffers)]
+    units = np.array([units_per_step(pool[pi]) for pi, _ in reqs])
+    budget = int(args.hbm_budget_gb * (1 << 30))
+    st16 = STORAGE[args.storage]
+
+    def summary(lat, makespan):
+        l = np.array([x[0] for x in lat])
+        q = np.array([x[1] for x in lat])
+        return {"p50_s": float(np.percentile(l, 50)), "p99_s": float(np.percentile(l, 99)),
+                "mean_s": float(l.mean()), "max_s": float(l.max()), "queued_p99_s": float(np.percentile(q, 99)),
+                "makespan_s": makespan, "GVoxel_tilt_per_s": float(units.sum() / makespan / 1e9),
+                "series_per_s": n / makespan}
+
+    # warm: one request of every pool series through each form
+    for storage, inflight in ((st16, args.inflight), (STORAGE["f32"], 1)):
+        w_reqs = [(i, False) for i in range(len(pool))]
+        serve_once(pool, frames, w_reqs, np.zeros(len(pool)), storage, inflight, budget, out_bufs)
+    clocks = ClockSampler(0)
+    clocks.start()
+    res = {}
+    zeros = np.zeros(n)
+    for name, storage, inflight in (("served", st16, args.inflight), ("plain_fp32", STORAGE["f32"], 1)):
+        res[name] = {"arrivals": summary(*serve_once(pool, frames, reqs, arrivals, storage, inflight, budget,
+                                                     out_bufs)),
+                     "saturated": summary(*serve_once(pool, frames, reqs, zeros, storage, inflight, budget,
+                                                      out_bufs))}
+    clk = clocks.stop()
+    # error against the FP64 oracle on two slices of one WBP and one SART series, each form
+    err = {}
+    if not args.no_cpu_baseline:
+        ol = _oracle()
+        k = int(np.argmin([c["nx"] * c["ny"] * c["vol_z"] for c in pool]))
+        c = pool[k]
+        y0 = c["ny"] // 2
+        for meth, kw in (("wbp", dict(method=0)), ("sart", dict(method=1, iterations=10, subsets=5))):
+            if meth == "sart":
+                ref = ol.sart(frames[k], c["tilts"], c["vol_z"], 0, len(c["tilts"]), 10, 5, y0=y0, y1=y0 + 2)
+            else:
+                ref = ol.wbp(frames[k], c["tilts"], c["vol_z"], y0=y0, y1=y0 + 2)
+            for sname, s in (("served", st16), ("plain_fp32", 0)):
+                srv = recon.Server(hbm_budget_bytes=budget, max_inflight=1)
+                rid = srv.submit(frames[k], c["tilts"], c["vol_z"], storage=s, **kw)
+                vol = srv.wait(rid)[0]
+                srv.close()
+                got = vol[y0:y0 + 2].astype(np.float64)
+                err[f"{meth}_{sname}"] = {"rel_l2": float(np.linalg.norm(got - ref) / np.linalg.norm(ref)),
+                                          "max_abs": float(np.abs(got - ref).max())}
+    sat = res["served"]["saturated"]["GVoxel_tilt_per_s"]
+    line = {"metric": METRIC, "value": sat, "unit": UNIT, "n_gpus": 1, "steps": n, "warmup": len(pool),
+            "ms_per_step": res["served"]["saturated"]["makespan_s"] / n * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": f"{args.storage}-storage/f32-accumulate",
+            "data": "synthetic",
+            "config": {"workload": f"serving: {n} requests over {len(pool)} distinct seeded series (nx, ny in "
+                                   f"256..1024 step 128, 31..61 tilts, thickness 64..300), Poisson arrivals "
+                                   f"mean {args.interarrival} s (20 s acquisition interval accelerated "
+                                   f"{20.0 / args.interarrival:.0f}x), 70% WBP / 30% SART 10 iterations 5 subsets, "
+                                   f"{args.storage} storage, {args.inflight} in flight, HBM budget "
+                                   f"{args.hbm_budget_gb} GB; host frames in, host volumes out",
+                       "name": "serve_mix", "step": "one request"},
+            "latency": res["served"]["arrivals"], "saturated": res["served"]["saturated"],
+            "plain_fp32": res["plain_fp32"],
+            "speedup_vs_plain_fp32": sat / res["plain_fp32"]["saturated"]["GVoxel_tilt_per_s"],
+            "p99_below_acquisition_interval": res["served"]["arrivals"]["p99_s"] < 20.0,
+            "e2e": {"value": sat, "unit": UNIT, "h2d_bytes_per_step": int(np.mean([frames[pi].nbytes for pi, _ in reqs])),
+                    "d2h_bytes_per_step": int(np.mean([4 * pool[pi]["ny"] * pool[pi]["vol_z"] * (pool[pi]["nx"] & ~1)
+                                                       for pi, _ in reqs]))},
+            "error": err, "clocks": clk}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -380,7 +626,24 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--storage", default="f32", choices=sorted(STORAGE),
                     help="staged-sinogram storage: f32, or f16 / bf16 with per-tilt scale (FP32 accumulation)")
+    ap.add_argument("--series", type=int, default=64, help="batch_uneven: number of series")
+    ap.add_argument("--group", type=int, default=16, help="batch_uneven: series resident per graph launch")
+    ap.add_argument("--branches", type=int, default=4, help="batch_uneven: parallel graph branches")
+    ap.add_argument("--requests", type=int, default=200, help="serve_mix: number of requests")
+    ap.add_argument("--pool", type=int, default=16, help="serve_mix: distinct series the requests draw from")
+    ap.add_argument("--interarrival", type=float, default=0.2, help="serve_mix: mean Poisson inter-arrival, s")
+    ap.add_argument("--inflight", type=int, default=4, help="serve_mix: requests on the GPU at once")
+    ap.add_argument("--out-buffers", type=int, default=12, help="serve_mix: pinned host volume buffers")
+    ap.add_argument("--hbm-budget-gb", type=float, default=150.0, help="serve_mix: HBM admission budget")
     args = ap.parse_args()
+    if args.impl == "ours" and args.workload in ("batch_uneven", "serve_mix"):
+        if args.workload == "batch_uneven":
+            run_batch_arm(args)
+        else:
+            if args.storage == "f32":
+                args.storage = "f16"
+            run_serving_arm(args)
+        return
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
     local_rank = int(os.environ.get("LOCAL_RANK", 0))

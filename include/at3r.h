@@ -136,9 +136,11 @@ at3r_status at3r_sart_device_noalloc(const float* proj, int nx, int ny, int n_ti
                                      int vol_z, int start_tilt, int num_tilts, int iterations, int subsets,
                                      float relax, float* vol, void* stream);
 
-/* Slab autotuner: times at3r_run_device with slab sizes from 4 slices up to
- * the plan's workspace capacity (doubling) on proj / vol (device buffers in
- * the layouts above, overwritten) and keeps the fastest for the plan.  The
+/* Slab autotuner: times the reconstruction of the leading rows (at most two
+ * full-capacity slabs) with slab sizes from 4 slices up to the plan's
+ * workspace capacity (doubling) on proj / vol (device buffers in the layouts
+ * above; those rows of vol are overwritten) and keeps the fastest for the
+ * plan.  The
  * choice is cached per problem shape, so later plans of the same shape skip
  * the timing.  *chosen (may be NULL) receives the slab. */
 at3r_status at3r_plan_autotune(at3r_plan* plan, const float* proj, float* vol, void* stream, int* chosen);
