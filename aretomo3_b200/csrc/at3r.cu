@@ -205,9 +205,9 @@ int probe_cufft_c2r(int nz, int nx)
 int round_up(int a, int b) { return (a + b - 1) / b * b; }
 
 enum KernelKind { KK_GATHER, KK_RWEIGHT, KK_BP_SART, KK_BP_WBP, KK_FP_DIFF, KK_FILL, KK_ROW_R2C, KK_ZCROP, KK_XC2R,
-                  KK_COUNT };
+                  KK_UNGROUP, KK_COUNT };
 const char* kKernelNames[KK_COUNT] = {"gather_weight", "rweight", "bp_sart", "bp_wbp_2x", "fp_diff",
-                                      "fill_empty", "row_r2c", "zcrop", "x_c2r"};
+                                      "fill_empty", "row_r2c", "zcrop", "x_c2r", "ungroup"};
 struct KStat {
     int64_t launches;
     double bytes, units, ms;
@@ -234,6 +234,7 @@ struct at3r_plan {
     void* d_raw = nullptr;
     void* d_diff = nullptr;
     void* d_shadow = nullptr;   // 16-bit storage: the volume shadow the forward projector reads
+    float4* d_w = nullptr;      // SART working volume, slice groups [ceil(S/4)][Nz][Nx] x 4 slices
     int* d_flags = nullptr;
     double* d_rf = nullptr;
     std::vector<double> h_rf;
@@ -398,18 +399,20 @@ at3r_status run_slab_t(at3r_plan* p, const float* proj, size_t tilt_stride, int 
         k_gather_weight<ST><<<dim3(T, S), 256, 0, st>>>(proj, tilt_stride, p->nx, proj_y0, p->d_cs, T, N, Nz, raw,
                                                         p->d_scale, p->d_flags);
         TE(p, st, KK_GATHER, (f4 + es) * S * T * N, (double)S * T * N);
-        AT3R_CUDA(cudaMemsetAsync(vol, 0, sizeof(float) * (size_t)S * Nx * Nz, st));
-        if (p->d_shadow)
-            AT3R_CUDA(cudaMemsetAsync(p->d_shadow, 0, 2 * (size_t)((S + 1) & ~1) * Nx * Nz, st));
+        // the working volume in slice groups: one 16-byte (or 8-byte shadow)
+        // load gives a tap of four slices; unpacked into vol at the end
+        AT3R_CUDA(cudaMemsetAsync(p->d_w, 0, sizeof(float4) * (size_t)SG * Nx * Nz, st));
+        if (p->d_shadow) AT3R_CUDA(cudaMemsetAsync(p->d_shadow, 0, sizeof(uint2) * (size_t)SG * Nx * Nz, st));
         BpArgs a{};
         a.T = T; a.N = N; a.cs = p->d_cs; a.GX = Nx; a.GZ = Nz; a.S = S;
-        a.out = vol; a.out_slice = (size_t)Nx * Nz; a.ww = p->bp_ww_sart; a.flags = p->d_flags;
+        a.out = reinterpret_cast<float*>(p->d_w); a.out_slice = (size_t)Nx * Nz; a.ww = p->bp_ww_sart;
+        a.flags = p->d_flags;
         a.scale = p->d_scale; a.shadow = p->d_shadow;
         const dim3 bgrid((Nx + BP_TX - 1) / BP_TX, (Nz + BP_TZ - 1) / BP_TZ, SG);
         // first back-projection: all tilts, relax 1 (CTomoSart.cpp:68-69)
         a.sino = raw; a.t0 = 0; a.t1 = T; a.relax = 1.f; a.low_bit = kFlagRawLow;
         TB(p, st);
-        k_bp<0, ST, VT><<<bgrid, BP_THREADS, bp_smem(T, a.ww), st>>>(a);
+        k_bp<0, ST, VT, true><<<bgrid, BP_THREADS, bp_smem(T, a.ww), st>>>(a);
         TE(p, st, KK_BP_SART, es * S * (double)T * N + (2 * f4 + (vs < 4 ? vs : 0)) * vox, vox * T);
         a.sino = dif; a.relax = p->relax; a.low_bit = kFlagDiffLow;
         for (int it = 0; it < p->g.iterations; it++) {
@@ -420,15 +423,20 @@ at3r_status run_slab_t(at3r_plan* p, const float* proj, size_t tilt_stride, int 
                 for (int t = t0; t < t0 + nt; t++) samples += (double)p->ray_len[t];
                 double* rfp = p->g.compute_rfactor ? p->d_rf + 2 * it : nullptr;
                 TB(p, st);
-                k_fp_diff<ST, VT><<<dim3((N + 255) / 256, nt, SG), 256, 0, st>>>(
-                    vol, p->d_shadow, Nx, Nz, S, raw, dif, p->d_scale, p->d_cs, T, N, t0, rfp, p->d_flags);
+                k_fp_diff<ST, VT, true><<<dim3((N + 255) / 256, nt, SG), 256, 0, st>>>(
+                    reinterpret_cast<const float*>(p->d_w), p->d_shadow, Nx, Nz, S, raw, dif, p->d_scale, p->d_cs, T,
+                    N, t0, rfp, p->d_flags);
                 TE(p, st, KK_FP_DIFF, vs * vox + 2.0 * es * S * nt * N, samples * N * S);
                 a.t0 = t0; a.t1 = t0 + nt;
                 TB(p, st);
-                k_bp<0, ST, VT><<<bgrid, BP_THREADS, bp_smem(nt, a.ww), st>>>(a);
+                k_bp<0, ST, VT, true><<<bgrid, BP_THREADS, bp_smem(nt, a.ww), st>>>(a);
                 TE(p, st, KK_BP_SART, es * S * (double)nt * N + (2 * f4 + (vs < 4 ? vs : 0)) * vox, vox * nt);
             }
         }
+        TB(p, st);
+        k_ungroup<<<dim3((unsigned)(((size_t)Nx * Nz + 255) / 256), SG), 256, 0, st>>>(p->d_w, vol, S,
+                                                                                       (size_t)Nx * Nz);
+        TE(p, st, KK_UNGROUP, 2 * f4 * vox, vox);
         TB(p, st);
         k_fill_empty<<<S, 256, 0, st>>>(vol, (size_t)Nx * Nz, p->d_flags);
         TE(p, st, KK_FILL, f4 * S, 0);
@@ -446,7 +454,7 @@ at3r_status run_slab_t(at3r_plan* p, const float* proj, size_t tilt_stride, int 
     a.ww = p->bp_ww_wbp; a.flags = p->d_flags; a.low_bit = kFlagRawLow;
     const dim3 bgrid((2 * Nx + BP_TX - 1) / BP_TX, (2 * Nz + BP_TZ - 1) / BP_TZ, SG);
     TB(p, st);
-    k_bp<1, ST, float><<<bgrid, BP_THREADS, bp_smem(T, a.ww), st>>>(a);
+    k_bp<1, ST, float, false><<<bgrid, BP_THREADS, bp_smem(T, a.ww), st>>>(a);
     TE(p, st, KK_BP_WBP, es * S * (double)T * N + f4 * 4 * vox, 4 * vox * T);
     TB(p, st);
     k_row_r2c<<<dim3(Nz, S), 512, p->smem_row, st>>>(p->d_g2, Nx, Nz, p->f2x.plan, p->d_y);
@@ -540,7 +548,7 @@ size_t at3r_plan_estimate_bytes(const at3r_geom* g)
     slab = std::min<size_t>(slab, (size_t)g->ny);
     size_t work;
     if (g->method == AT3R_SART)
-        work = slab * (2 * T * N * esz + (esz < 4 ? 2 * Nx * Nz + T * 4 : 0)) + slab * 8;
+        work = (slab + 3) * (2 * T * N * esz + 4 * Nx * Nz + (esz < 4 ? 2 * Nx * Nz + T * 4 : 0)) + slab * 8;
     else
         work = slab * (T * N * esz + 16 * Nx * Nz + 2 * Nz * KX * sizeof(float2) + (esz < 4 ? T * 4 : 0) + 4);
     const size_t host_path = 2 * (T * slab * nx + slab * Nx * Nz) * sizeof(float);
@@ -611,8 +619,8 @@ at3r_status plan_create_impl(const at3r_geom* g, cudaStream_t alloc_stream, at3r
         for (int i = 1; i < k; i++) p->sub_start[i] = p->sub_start[i - 1] + p->sub_size[i - 1];
         p->bp_ww_sart = bp_window(BP_TX, BP_TZ, 1.0, cs, p->T);
         if (p->bp_ww_sart > BP_WW) return fail(set_err(AT3R_ERR_TOO_LARGE, "back-projection window exceeds its stride"));
-        for (const void* fn : {(const void*)k_bp<0, float, float>, (const void*)k_bp<0, __half, __half>,
-                               (const void*)k_bp<0, __nv_bfloat16, __nv_bfloat16>})
+        for (const void* fn : {(const void*)k_bp<0, float, float, true>, (const void*)k_bp<0, __half, __half, true>,
+                               (const void*)k_bp<0, __nv_bfloat16, __nv_bfloat16, true>})
             if ((rc = set_smem(fn, bp_smem(p->T, p->bp_ww_sart)))) return fail(rc);
         per_slice = 2 * T * N * sizeof(float) + Nx * Nz * sizeof(float);
     } else {
@@ -637,8 +645,8 @@ at3r_status plan_create_impl(const at3r_geom* g, cudaStream_t alloc_stream, at3r
         if ((rc = set_smem((const void*)k_row_r2c, p->smem_row))) return fail(rc);
         if ((rc = set_smem((const void*)k_zcrop, p->smem_zcrop))) return fail(rc);
         if ((rc = set_smem((const void*)k_x_c2r, p->smem_xc2r))) return fail(rc);
-        for (const void* fn : {(const void*)k_bp<1, float, float>, (const void*)k_bp<1, __half, float>,
-                               (const void*)k_bp<1, __nv_bfloat16, float>})
+        for (const void* fn : {(const void*)k_bp<1, float, float, false>, (const void*)k_bp<1, __half, float, false>,
+                               (const void*)k_bp<1, __nv_bfloat16, float, false>})
             if ((rc = set_smem(fn, bp_smem(p->T, p->bp_ww_wbp)))) return fail(rc);
         // R-weight transfer function (GRWeight.cu:15-20), 1/N folded in
         std::vector<float> h(N / 2 + 1);
@@ -668,8 +676,10 @@ at3r_status plan_create_impl(const at3r_geom* g, cudaStream_t alloc_stream, at3r
         if (g->storage != AT3R_STORE_F32) {
             if ((rc = dalloc(p, &p->d_scale, S * T))) return fail(rc);
             // slice pairs of 16-bit values, the slab rounded up to whole SB groups
-            if ((rc = dalloc_bytes(p, &p->d_shadow, 2 * ((S + SB - 1) / SB * SB) * Nx * Nz))) return fail(rc);
+            if ((rc = dalloc_bytes(p, &p->d_shadow, sizeof(uint2) * ((S + SB - 1) / SB) * Nx * Nz))) return fail(rc);
         }
+        if ((rc = dalloc_bytes(p, reinterpret_cast<void**>(&p->d_w), sizeof(float4) * ((S + SB - 1) / SB) * Nx * Nz)))
+            return fail(rc);
         if ((rc = dalloc(p, &p->d_flags, S))) return fail(rc);
         if ((rc = dalloc(p, &p->d_rf, 2 * (size_t)std::max(1, g->iterations)))) return fail(rc);
         p->h_rf.assign(2 * std::max(1, g->iterations), 0.0);
@@ -688,6 +698,7 @@ void at3r_plan_destroy(at3r_plan* p)
 {
     if (!p) return;
     for (void* ptr : {(void*)p->d_cs, (void*)p->d_raw, (void*)p->d_diff, (void*)p->d_scale, (void*)p->d_shadow,
+                      (void*)p->d_w,
                       (void*)p->d_flags, (void*)p->d_rf, (void*)p->d_h, (void*)p->d_filt, (void*)p->d_g2,
                       (void*)p->d_y})
         dfree(p, ptr);
@@ -883,7 +894,7 @@ at3r_status noalloc_scratch_address(unsigned char** out)
         return set_err(AT3R_ERR_CUDA, std::string("cudaGetSymbolAddress(no-allocation scratch): ") +
                                           cudaGetErrorString(e));
     }
-    at3r_status rc = set_smem((const void*)k_bp<0, float, float>, 0);
+    at3r_status rc = set_smem((const void*)k_bp<0, float, float, false>, 0);
     if (rc != AT3R_OK) return rc;
     addr[dev] = (unsigned char*)ptr;
     *out = (unsigned char*)ptr;
@@ -958,19 +969,19 @@ extern "C" at3r_status at3r_sart_device_noalloc(const float* proj, int nx, int n
         a.out = v; a.out_slice = (size_t)Nx * Nz; a.ww = ww; a.flags = d_flags;
         const dim3 bgrid((Nx + BP_TX - 1) / BP_TX, (Nz + BP_TZ - 1) / BP_TZ, SG);
         a.sino = d_raw; a.t0 = 0; a.t1 = T; a.relax = 1.f; a.low_bit = kFlagRawLow;
-        k_bp<0, float, float><<<bgrid, BP_THREADS, bp_smem(T, ww), st>>>(a);
+        k_bp<0, float, float, false><<<bgrid, BP_THREADS, bp_smem(T, ww), st>>>(a);
         AT3R_CUDA(cudaGetLastError());
         a.sino = d_diff; a.relax = rlx; a.low_bit = kFlagDiffLow;
         for (int it = 0; it < iterations; it++) {
             for (int s = 0; s < subsets; s++) {
                 const int t0 = sub_start[s] + start_tilt, nt = sub_size[s];
                 if (nt <= 0) continue;
-                k_fp_diff<float, float><<<dim3((N + 255) / 256, nt, SG), 256, 0, st>>>(v, nullptr, Nx, Nz, S, d_raw, d_diff,
+                k_fp_diff<float, float, false><<<dim3((N + 255) / 256, nt, SG), 256, 0, st>>>(v, nullptr, Nx, Nz, S, d_raw, d_diff,
                                                                                        nullptr, d_cs, T, N, t0, nullptr,
                                                                                        d_flags);
                 AT3R_CUDA(cudaGetLastError());
                 a.t0 = t0; a.t1 = t0 + nt;
-                k_bp<0, float, float><<<bgrid, BP_THREADS, bp_smem(nt, ww), st>>>(a);
+                k_bp<0, float, float, false><<<bgrid, BP_THREADS, bp_smem(nt, ww), st>>>(a);
                 AT3R_CUDA(cudaGetLastError());
             }
         }

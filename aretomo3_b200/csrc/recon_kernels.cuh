@@ -76,6 +76,68 @@ struct Pair<__nv_bfloat16> {
     __device__ __forceinline__ static __nv_bfloat16 one(float a) { return __float2bfloat16_rn(a); }
 };
 
+// Four slices of the SART working volume at one voxel (the slice-group
+// layout): FP32 as float4; the 16-bit shadow as four 16-bit values in 8 bytes.
+template <typename VT>
+struct Quad;
+template <>
+struct Quad<float> {
+    using T4 = float4;
+    __device__ __forceinline__ static float4 ld(const float4* p) { return __ldg(p); }
+};
+template <typename T2>
+__device__ __forceinline__ uint32_t bits_of(T2 v)
+{
+    return *reinterpret_cast<uint32_t*>(&v);
+}
+template <typename T2>
+__device__ __forceinline__ T2 from_bits(uint32_t u)
+{
+    return *reinterpret_cast<T2*>(&u);
+}
+template <>
+struct Quad<__half> {
+    using T4 = uint2;
+    __device__ __forceinline__ static float4 ld(const uint2* p)
+    {
+        const uint2 u = __ldg(p);
+        const float2 a = __half22float2(from_bits<__half2>(u.x)), b = __half22float2(from_bits<__half2>(u.y));
+        return make_float4(a.x, a.y, b.x, b.y);
+    }
+    __device__ __forceinline__ static uint2 make(float4 v)
+    {
+        return make_uint2(bits_of(__floats2half2_rn(v.x, v.y)), bits_of(__floats2half2_rn(v.z, v.w)));
+    }
+    __device__ __forceinline__ static void st1(uint2* p, int q, float v)
+    {
+        reinterpret_cast<__half*>(p)[q] = __float2half_rn(v);
+    }
+};
+template <>
+struct Quad<__nv_bfloat16> {
+    using T4 = uint2;
+    __device__ __forceinline__ static float4 ld(const uint2* p)
+    {
+        const uint2 u = __ldg(p);
+        const float2 a = __bfloat1622float2(from_bits<__nv_bfloat162>(u.x));
+        const float2 b = __bfloat1622float2(from_bits<__nv_bfloat162>(u.y));
+        return make_float4(a.x, a.y, b.x, b.y);
+    }
+    __device__ __forceinline__ static uint2 make(float4 v)
+    {
+        return make_uint2(bits_of(__floats2bfloat162_rn(v.x, v.y)), bits_of(__floats2bfloat162_rn(v.z, v.w)));
+    }
+    __device__ __forceinline__ static void st1(uint2* p, int q, float v)
+    {
+        reinterpret_cast<__nv_bfloat16*>(p)[q] = __float2bfloat16_rn(v);
+    }
+};
+
+__device__ __forceinline__ float comp(const float4& v, int q)
+{
+    return q == 0 ? v.x : q == 1 ? v.y : q == 2 ? v.z : v.w;
+}
+
 // Largest magnitude over a CTA's values (non-empty ones only); every thread
 // gets the result.  Uses red[32] of shared memory.
 __device__ __forceinline__ float block_absmax(float v, float* red)
@@ -242,12 +304,14 @@ struct BpArgs {
     int GX, GZ;              // voxel grid of this mode
     int S;                   // slices in this launch
     float relax;
-    float* out;              // MODE 0: vol slab [slices][GZ][GX] (z flipped); MODE 1: [slices][GZ][GX]
+    float* out;              // MODE 0: vol slab [slices][GZ][GX] (z flipped), or the slice-group volume
+                             // [groups][GZ][GX] float4; MODE 1: [slices][GZ][GX]
     size_t out_slice;
     int ww;                  // staged window width (samples)
     int* flags;              // per-slice flag bits
     int low_bit;             // the flag bit that marks this sinogram as holding low values
-    void* shadow;            // MODE 0, 16-bit volume type: [ceil(slices/2)][GZ][GX] slice pairs (z flipped)
+    void* shadow;            // MODE 0, 16-bit volume type: [ceil(slices/2)][GZ][GX] slice pairs (z flipped),
+                             // or [groups][GZ][GX] of four 16-bit values beside the slice-group volume
 };
 
 template <int MODE>
@@ -306,9 +370,66 @@ __device__ __forceinline__ void shadow_one(const BpArgs& p, int ys, int Z, int X
     *sh = Pair<VT>::one(a);
 }
 
-template <int MODE, typename ST, typename VT>
+// SART update of one voxel of the slice-group working volume
+// ([groups][GZ][GX] float4, component q = slice 4g + q, rows z flipped): all
+// four slices at once, and the 16-bit shadow beside it.  Components past the
+// slab's last slice are computed from zero rows and never read back.
+static_assert(SB == 4, "the slice-group layout holds four slices per voxel");
+template <typename VT>
+__device__ __forceinline__ void bp_store_grp(const BpArgs& p, int g, int ys0, int nsl, int Z, int X, float4 sum,
+                                             int cnt)
+{
+    if (cnt <= 0) return;
+    const size_t idx = ((size_t)g * p.GZ + (p.GZ - 1 - Z)) * p.GX + X;
+    float4* v4 = reinterpret_cast<float4*>(p.out) + idx;
+    const float4 o = *v4;
+    const float rc = (float)cnt;
+    const float sm[4] = {sum.x, sum.y, sum.z, sum.w}, old[4] = {o.x, o.y, o.z, o.w};
+    float r[4];
+    int empty = 0;
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+        const float f = __fadd_rn(__fdiv_rn(__fmul_rn(p.relax, sm[q]), rc), old[q]);
+        if (f > kSentinelTest) {
+            r[q] = fmaxf(f, 0.f);
+        } else {
+            r[q] = kSentinelValue;
+            if (q < nsl) empty |= 1 << q;
+        }
+    }
+    const float4 nv = make_float4(r[0], r[1], r[2], r[3]);
+    *v4 = nv;
+    if (empty) {
+#pragma unroll
+        for (int q = 0; q < 4; q++)
+            if ((empty >> q) & 1) atomicOr(p.flags + ys0 + q, kFlagVolEmpty);
+    }
+    if constexpr (!std::is_same<VT, float>::value) reinterpret_cast<uint2*>(p.shadow)[idx] = Quad<VT>::make(nv);
+}
+template <typename VT>
+__device__ __forceinline__ void bp_store1_grp(const BpArgs& p, int g, int q, int ys, int Z, int X, float sum, int cnt)
+{
+    if (cnt <= 0) return;
+    const size_t idx = ((size_t)g * p.GZ + (p.GZ - 1 - Z)) * p.GX + X;
+    float* v = reinterpret_cast<float*>(p.out) + 4 * idx + q;
+    const float f = __fadd_rn(__fdiv_rn(__fmul_rn(p.relax, sum), (float)cnt), *v);
+    float r;
+    if (f > kSentinelTest) {
+        r = fmaxf(f, 0.f);
+    } else {
+        r = kSentinelValue;
+        atomicOr(p.flags + ys, kFlagVolEmpty);
+    }
+    *v = r;
+    if constexpr (!std::is_same<VT, float>::value) Quad<VT>::st1(reinterpret_cast<uint2*>(p.shadow) + idx, q, r);
+}
+
+// GRP (MODE 0 only): the volume is the slice-group working volume above;
+// otherwise MODE 0 updates a plain [slices][GZ][GX] volume (z flipped).
+template <int MODE, typename ST, typename VT, bool GRP>
 __global__ void __launch_bounds__(BP_THREADS) k_bp(BpArgs p)
 {
+    static_assert(!GRP || MODE == 0, "the slice-group layout is the SART working volume");
     extern __shared__ float2 bsm[];
     float2* cs_s = bsm;                                               // [BP_CHUNK]
     float2* pw = bsm + BP_CHUNK;                                      // [SB][BP_CHUNK][BP_WW]
@@ -371,6 +492,11 @@ __global__ void __launch_bounds__(BP_THREADS) k_bp(BpArgs p)
     };
 
     if (!low) {
+        if (GRP && nsl < SB) {
+            // rows of slices past the slab's end stay zero (staging never writes them)
+            for (int k = threadIdx.x; k < (SB - nsl) * BP_PSLAB; k += BP_THREADS)
+                pw[nsl * BP_PSLAB + k] = make_float2(0.f, 0.f);
+        }
         float sum[SB][BP_CZ][BP_CX];
         int cnt[BP_CZ][BP_CX];
 #pragma unroll
@@ -448,14 +574,19 @@ __global__ void __launch_bounds__(BP_THREADS) k_bp(BpArgs p)
             for (int i = 0; i < BP_CX; i++) {
                 const int X = X0 + lane + 32 * i;
                 if (Z >= p.GZ || X >= p.GX) continue;
-                float nv[SB];
+                if constexpr (GRP) {
+                    bp_store_grp<VT>(p, blockIdx.z, ys0, nsl, Z, X,
+                                     make_float4(sum[0][j][i], sum[1][j][i], sum[2][j][i], sum[3][j][i]), cnt[j][i]);
+                } else {
+                    float nv[SB];
 #pragma unroll
-                for (int q = 0; q < SB; q++)
-                    nv[q] = q < nsl ? bp_store<MODE>(p, ys0 + q, Z, X, sum[q][j][i], cnt[j][i]) : 0.f;
-                if constexpr (MODE == 0 && !std::is_same<VT, float>::value) {
+                    for (int q = 0; q < SB; q++)
+                        nv[q] = q < nsl ? bp_store<MODE>(p, ys0 + q, Z, X, sum[q][j][i], cnt[j][i]) : 0.f;
+                    if constexpr (MODE == 0 && !std::is_same<VT, float>::value) {
 #pragma unroll
-                    for (int g = 0; g < SB / 2; g++)
-                        if (2 * g < nsl) shadow_pair<VT>(p, ys0 + 2 * g, Z, X, nv[2 * g], nv[2 * g + 1]);
+                        for (int g = 0; g < SB / 2; g++)
+                            if (2 * g < nsl) shadow_pair<VT>(p, ys0 + 2 * g, Z, X, nv[2 * g], nv[2 * g + 1]);
+                    }
                 }
             }
         }
@@ -503,8 +634,12 @@ __global__ void __launch_bounds__(BP_THREADS) k_bp(BpArgs p)
             for (int i = 0; i < BP_CX; i++) {
                 const int X = X0 + lane + 32 * i;
                 if (Z < p.GZ && X < p.GX) {
-                    const float nv = bp_store<MODE>(p, ys0 + q, Z, X, sum[j][i], cnt[j][i]);
-                    if constexpr (MODE == 0 && !std::is_same<VT, float>::value) shadow_one<VT>(p, ys0 + q, Z, X, nv);
+                    if constexpr (GRP) {
+                        bp_store1_grp<VT>(p, blockIdx.z, q, ys0 + q, Z, X, sum[j][i], cnt[j][i]);
+                    } else {
+                        const float nv = bp_store<MODE>(p, ys0 + q, Z, X, sum[j][i], cnt[j][i]);
+                        if constexpr (MODE == 0 && !std::is_same<VT, float>::value) shadow_one<VT>(p, ys0 + q, Z, X, nv);
+                    }
                 }
             }
         }
@@ -585,9 +720,12 @@ __device__ __forceinline__ float bilerp(float a00, float a10, float a01, float a
 }
 
 // ST: storage of raw / diff rows; VT: float reads the FP32 volume, __half /
-// __nv_bfloat16 read its 16-bit shadow (two slices per word) — the FP32
-// volume is then read only for slices that may hold "empty" voxels.
-template <typename ST, typename VT>
+// __nv_bfloat16 read its 16-bit shadow — the FP32 volume is then read only
+// for slices that may hold "empty" voxels.  GRP: the volume (and shadow) are
+// in the slice-group layout, so one load gives a tap of all four slices;
+// otherwise the volume is plain [slices][Nz][Nx] and the shadow holds slice
+// pairs.
+template <typename ST, typename VT, bool GRP>
 __global__ void __launch_bounds__(256) k_fp_diff(const float* __restrict__ vol, const void* __restrict__ shadow,
                                                  int Nx, int Nz, int S, const ST* __restrict__ raw,
                                                  ST* __restrict__ diff, const float* __restrict__ scale,
@@ -614,7 +752,33 @@ __global__ void __launch_bounds__(256) k_fp_diff(const float* __restrict__ vol, 
 #pragma unroll
     for (int q = 0; q < SB; q++) { fSum[q] = 0.f; fCount[q] = 0.f; }
     bool shadow_done = false;
-    if constexpr (!std::is_same<VT, float>::value) {
+    if constexpr (GRP) {
+      if (!empty_vox) {
+        shadow_done = true;
+        // slice group: one load per tap; rows of voxel Z and Z + 1 as bases
+        using T4 = typename Quad<VT>::T4;
+        const T4* g0 = (std::is_same<VT, float>::value ? reinterpret_cast<const T4*>(vol)
+                                                        : reinterpret_cast<const T4*>(shadow)) +
+                       (size_t)blockIdx.z * slice + (size_t)(Nz - 1) * Nx;
+        const T4* g1 = g0 - Nx;
+        for (int i = wlo; i <= whi; i++) {
+            if (i < lo || i > hi) continue;
+            const float fX = r.x(i), fZ = r.z(i);
+            const int iX = (int)fX, iZ = (int)fZ;
+            const float wx = fX - (float)iX, wz = fZ - (float)iZ;
+            const int o = iX - iZ * Nx;
+            const float4 a00 = Quad<VT>::ld(g0 + o), a10 = Quad<VT>::ld(g0 + o + 1);
+            const float4 a01 = Quad<VT>::ld(g1 + o), a11 = Quad<VT>::ld(g1 + o + 1);
+            fSum[0] += bilerp(a00.x, a10.x, a01.x, a11.x, wx, wz);
+            fSum[1] += bilerp(a00.y, a10.y, a01.y, a11.y, wx, wz);
+            fSum[2] += bilerp(a00.z, a10.z, a01.z, a11.z, wx, wz);
+            fSum[3] += bilerp(a00.w, a10.w, a01.w, a11.w, wx, wz);
+        }
+        const float n = (float)max(hi - lo + 1, 0);
+#pragma unroll
+        for (int q = 0; q < SB; q++) fCount[q] = n;
+      }
+    } else if constexpr (!std::is_same<VT, float>::value) {
       if (!empty_vox) {
         shadow_done = true;
         using T2 = typename Pair<VT>::T2;
@@ -674,16 +838,19 @@ __global__ void __launch_bounds__(256) k_fp_diff(const float* __restrict__ vol, 
 #pragma unroll
         for (int q = 0; q < SB; q++) fCount[q] = n;
     } else {
+        // element stride: 4 in the slice-group layout, 1 in the plain one
+        constexpr int E = GRP ? 4 : 1;
         for (int q = 0; q < nsl; q++) {
-            const float* v0 = vbase + (size_t)(ys0 + q) * slice;
+            const float* v0 = GRP ? vol + E * ((size_t)blockIdx.z * slice + (size_t)(Nz - 1) * Nx) + q
+                                  : vbase + (size_t)(ys0 + q) * slice;
             float s0 = 0.f, n0 = 0.f;
             for (int i = wlo; i <= whi; i++) {
                 if (i < lo || i > hi) continue;
                 const float fX = r.x(i), fZ = r.z(i);
                 const int iX = (int)fX, iZ = (int)fZ;
-                const float* p = v0 + iX - (ptrdiff_t)iZ * Nx;
-                const float val = bilerp(__ldg(p), __ldg(p + 1), __ldg(p - Nx), __ldg(p - Nx + 1), fX - (float)iX,
-                                         fZ - (float)iZ);
+                const float* p = v0 + E * (iX - (ptrdiff_t)iZ * Nx);
+                const float val = bilerp(__ldg(p), __ldg(p + E), __ldg(p - E * Nx), __ldg(p - E * Nx + E),
+                                         fX - (float)iX, fZ - (float)iZ);
                 if (val < kSentinelTest) continue;
                 s0 += val;
                 n0 += 1.f;
@@ -731,6 +898,26 @@ __global__ void __launch_bounds__(256) k_fp_diff(const float* __restrict__ vol, 
             atomicAdd(rf + 1, sr);
         }
     }
+}
+
+// ---------------------------------------------------------------------------
+// Slice-group working volume -> output slices: vol[4g + q][r][x] =
+// W[g][r][x].q for the slab's S slices (rows already z flipped).
+// Grid (ceil(Nx*Nz / 256), groups).
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_ungroup(const float4* __restrict__ w, float* __restrict__ vol, int S,
+                                                 size_t slice)
+{
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int g = blockIdx.y;
+    if (i >= slice) return;
+    const float4 v = __ldg(w + (size_t)g * slice + i);
+    const int n = min(4, S - 4 * g);
+    float* o = vol + (size_t)4 * g * slice + i;
+    o[0] = v.x;
+    if (n > 1) o[slice] = v.y;
+    if (n > 2) o[2 * slice] = v.z;
+    if (n > 3) o[3 * slice] = v.w;
 }
 
 // ---------------------------------------------------------------------------
