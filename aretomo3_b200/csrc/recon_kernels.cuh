@@ -22,6 +22,12 @@ namespace at3r {
 constexpr float kSentinelTest = -1e10f;   // "empty sample" threshold of the reference
 constexpr float kSentinelValue = -1e30f;  // value the reference writes for "no sample"
 
+// floor without the conversion units: for 0 <= x < 2^23, x + 2^23 rounded
+// down is 2^23 + floor(x) exactly, so its bit pattern minus kMagicBits is
+// floor(x) and subtracting 2^23 again gives floor(x) as a float.
+constexpr float kMagic = 8388608.0f;
+constexpr int kMagicBits = 0x4B000000;
+
 // ---------------------------------------------------------------------------
 // Storage of staged sinograms.  FP32 as is; FP16 / BF16 as value / scale with
 // one scale per (slice, tilt) row (the row's largest magnitude), so a row
@@ -285,14 +291,15 @@ __global__ void __launch_bounds__(512) k_rweight(const float* __restrict__ proj,
 // slices; a chunk whose tilts keep the whole tile strictly inside [0, N-2]
 // skips the test.  Slices whose staged data hold values near the -1e10
 // "empty" marker (flag bit) go through the per-slice path that tests every
-// sample as the reference does.  All paths add the same values in the same
-// (tilt) order.
+// sample as the reference does.  Sums run in the reference's (tilt) order;
+// the fast paths fold the lerp into the sum with fused multiply-adds.
 // ---------------------------------------------------------------------------
 constexpr int BP_TX = 64, BP_TZ = 32, BP_THREADS = 256, BP_CHUNK = 16;
 // Shared-memory stride of one tilt's staged window (pairs).  A window spans
-// at most (BP_TX - 1) + (BP_TZ - 1) + 6 = 100 samples (|cos|, |sin| <= 1), so
-// a fixed stride holds every case and makes the per-slice offsets immediates.
-constexpr int BP_WW = 128;
+// at most |cos|(BP_TX - 1) + |sin|(BP_TZ - 1) + 6 <= sqrt(63^2 + 31^2) + 6 < 77
+// samples (cos^2 + sin^2 = 1; the WBP grid halves it), so a fixed stride
+// holds every case and makes the per-slice offsets immediates.
+constexpr int BP_WW = 80;
 constexpr int BP_PSLAB = BP_CHUNK * BP_WW;   // pairs per slice
 constexpr int BP_CX = BP_TX / 32, BP_CZ = BP_TZ / (BP_THREADS / 32);
 
@@ -332,14 +339,16 @@ __host__ __device__ inline size_t bp_smem_bytes(int)
 
 // Writes one voxel and returns its value afterwards (the old value where no
 // tilt contributed).
+// k: relax / cnt (MODE 0) or 1 / cnt (MODE 1), one division per voxel for
+// all its slices.
 template <int MODE>
-__device__ __forceinline__ float bp_store(const BpArgs& p, int ys, int Z, int X, float sum, int cnt)
+__device__ __forceinline__ float bp_store(const BpArgs& p, int ys, int Z, int X, float sum, int cnt, float k)
 {
     float* out = p.out + (size_t)ys * p.out_slice;
     if (MODE == 0) {
         float* v = out + (size_t)(p.GZ - 1 - Z) * p.GX + X;
         if (cnt <= 0) return *v;
-        const float f = __fadd_rn(__fdiv_rn(__fmul_rn(p.relax, sum), (float)cnt), *v);
+        const float f = __fadd_rn(__fmul_rn(sum, k), *v);
         if (f > kSentinelTest) {
             const float r = fmaxf(f, 0.f);
             *v = r;
@@ -349,7 +358,7 @@ __device__ __forceinline__ float bp_store(const BpArgs& p, int ys, int Z, int X,
         atomicOr(p.flags + ys, kFlagVolEmpty);
         return kSentinelValue;
     } else {
-        const float r = cnt > 0 ? __fdiv_rn(sum, (float)cnt) : 0.f;
+        const float r = cnt > 0 ? __fmul_rn(sum, k) : 0.f;
         out[(size_t)Z * p.GX + X] = r;
         return r;
     }
@@ -383,13 +392,13 @@ __device__ __forceinline__ void bp_store_grp(const BpArgs& p, int g, int ys0, in
     const size_t idx = ((size_t)g * p.GZ + (p.GZ - 1 - Z)) * p.GX + X;
     float4* v4 = reinterpret_cast<float4*>(p.out) + idx;
     const float4 o = *v4;
-    const float rc = (float)cnt;
+    const float k = __fdiv_rn(p.relax, (float)cnt);
     const float sm[4] = {sum.x, sum.y, sum.z, sum.w}, old[4] = {o.x, o.y, o.z, o.w};
     float r[4];
     int empty = 0;
 #pragma unroll
     for (int q = 0; q < 4; q++) {
-        const float f = __fadd_rn(__fdiv_rn(__fmul_rn(p.relax, sm[q]), rc), old[q]);
+        const float f = __fadd_rn(__fmul_rn(sm[q], k), old[q]);
         if (f > kSentinelTest) {
             r[q] = fmaxf(f, 0.f);
         } else {
@@ -412,7 +421,7 @@ __device__ __forceinline__ void bp_store1_grp(const BpArgs& p, int g, int q, int
     if (cnt <= 0) return;
     const size_t idx = ((size_t)g * p.GZ + (p.GZ - 1 - Z)) * p.GX + X;
     float* v = reinterpret_cast<float*>(p.out) + 4 * idx + q;
-    const float f = __fadd_rn(__fdiv_rn(__fmul_rn(p.relax, sum), (float)cnt), *v);
+    const float f = __fadd_rn(__fmul_rn(sum, __fdiv_rn(p.relax, (float)cnt)), *v);
     float r;
     if (f > kSentinelTest) {
         r = fmaxf(f, 0.f);
@@ -427,7 +436,7 @@ __device__ __forceinline__ void bp_store1_grp(const BpArgs& p, int g, int q, int
 // GRP (MODE 0 only): the volume is the slice-group working volume above;
 // otherwise MODE 0 updates a plain [slices][GZ][GX] volume (z flipped).
 template <int MODE, typename ST, typename VT, bool GRP>
-__global__ void __launch_bounds__(BP_THREADS) k_bp(BpArgs p)
+__global__ void __launch_bounds__(BP_THREADS, 3) k_bp(BpArgs p)
 {
     static_assert(!GRP || MODE == 0, "the slice-group layout is the SART working volume");
     extern __shared__ float2 bsm[];
@@ -472,19 +481,29 @@ __global__ void __launch_bounds__(BP_THREADS) k_bp(BpArgs p)
             inside = (lo >= 0.01f) && (hi <= endX - 0.01f);
         }
         inside = __syncthreads_and(inside);
-        // one warp per (slice, tilt) row, lanes along the window
-        for (int row = warp; row < ns * nc; row += BP_THREADS / 32) {
+        // one warp per (slice, tilt) row, lanes along the window; a lane issues
+        // all its loads of the row before its first store, so a warp waits for
+        // the L2 once per row rather than once per load
+        constexpr int NW = BP_THREADS / 32, KS = (BP_WW + 31) / 32;
+        for (int row = warp; row < ns * nc; row += NW) {
             const int q = row / nc, t = row - q * nc;
             const int x0 = ws[t];
             const size_t row_id = (size_t)(ysA + q) * p.T + c0 + t;
             const ST* src = reinterpret_cast<const ST*>(p.sino) + row_id * p.N;
             const float sc = std::is_same<ST, float>::value ? 1.f : __ldg(p.scale + row_id);
             float2* dst = pw + q * BP_PSLAB + t * BP_WW;
-            for (int k = lane; k < p.ww; k += 32) {
-                const int x = x0 + k;
-                const float a = (x >= 0 && x < p.N) ? Stor<ST>::ld(src + x, sc) : 0.f;
-                const float b = (x + 1 >= 0 && x + 1 < p.N) ? Stor<ST>::ld(src + x + 1, sc) : 0.f;
-                dst[k] = make_float2(a, b);
+            float va[KS], vb[KS];
+#pragma unroll
+            for (int u = 0; u < KS; u++) {
+                const int k = lane + 32 * u, x = x0 + k;
+                const bool kv = k < p.ww;
+                va[u] = (kv && x >= 0 && x < p.N) ? Stor<ST>::ld(src + x, sc) : 0.f;
+                vb[u] = (kv && x + 1 >= 0 && x + 1 < p.N) ? Stor<ST>::ld(src + x + 1, sc) : 0.f;
+            }
+#pragma unroll
+            for (int u = 0; u < KS; u++) {
+                const int k = lane + 32 * u;
+                if (k < p.ww) dst[k] = make_float2(va[u], vb[u]);
             }
         }
         __syncthreads();
@@ -514,22 +533,22 @@ __global__ void __launch_bounds__(BP_THREADS) k_bp(BpArgs p)
                 // the whole tile lands inside the detector for every tilt of the chunk
                 for (int t = 0; t < nc; t++) {
                     const float2 c = cs_s[t];
-                    const float2* w = pw + t * BP_WW;
-                    const int st = ws[t];
+                    // window index of sample xp: floor(xp) - st, from the bits of xp + 2^23
+                    const int wb = t * BP_WW - ws[t] - kMagicBits;
 #pragma unroll
                     for (int j = 0; j < BP_CZ; j++) {
                         const float fzs = __fmul_rn(fZ[j], c.y);
 #pragma unroll
                         for (int i = 0; i < BP_CX; i++) {
                             const float xp = bp_xp<MODE>(fX[i], fzs, c.x, cent);
-                            const int ii = (int)xp;
-                            const float fr = __fsub_rn(xp, (float)ii);
+                            const float tr = __fadd_rd(xp, kMagic);
+                            const float fr = __fsub_rn(xp, __fsub_rn(tr, kMagic));
                             const float om = __fsub_rn(1.f, fr);
-                            const float2* wq = w + min((unsigned)(ii - st), wmax);
+                            const float2* wq = pw + (__float_as_int(tr) + wb);
 #pragma unroll
                             for (int q = 0; q < SB; q++) {
                                 const float2 v = wq[q * BP_PSLAB];
-                                sum[q][j][i] = __fadd_rn(sum[q][j][i], __fmaf_rn(v.x, om, __fmul_rn(v.y, fr)));
+                                sum[q][j][i] = __fmaf_rn(v.y, fr, __fmaf_rn(v.x, om, sum[q][j][i]));
                             }
                         }
                     }
@@ -557,8 +576,8 @@ __global__ void __launch_bounds__(BP_THREADS) k_bp(BpArgs p)
 #pragma unroll
                             for (int q = 0; q < SB; q++) {
                                 const float2 v = wq[q * BP_PSLAB];
-                                const float add = __fmaf_rn(v.x, om, __fmul_rn(v.y, fr));
-                                sum[q][j][i] = in ? __fadd_rn(sum[q][j][i], add) : sum[q][j][i];
+                                const float acc = __fmaf_rn(v.y, fr, __fmaf_rn(v.x, om, sum[q][j][i]));
+                                sum[q][j][i] = in ? acc : sum[q][j][i];
                             }
                             cnt[j][i] += in ? 1 : 0;
                         }
@@ -579,9 +598,10 @@ __global__ void __launch_bounds__(BP_THREADS) k_bp(BpArgs p)
                                      make_float4(sum[0][j][i], sum[1][j][i], sum[2][j][i], sum[3][j][i]), cnt[j][i]);
                 } else {
                     float nv[SB];
+                    const float k = cnt[j][i] > 0 ? __fdiv_rn(MODE == 0 ? p.relax : 1.f, (float)cnt[j][i]) : 0.f;
 #pragma unroll
                     for (int q = 0; q < SB; q++)
-                        nv[q] = q < nsl ? bp_store<MODE>(p, ys0 + q, Z, X, sum[q][j][i], cnt[j][i]) : 0.f;
+                        nv[q] = q < nsl ? bp_store<MODE>(p, ys0 + q, Z, X, sum[q][j][i], cnt[j][i], k) : 0.f;
                     if constexpr (MODE == 0 && !std::is_same<VT, float>::value) {
 #pragma unroll
                         for (int g = 0; g < SB / 2; g++)
@@ -637,7 +657,8 @@ __global__ void __launch_bounds__(BP_THREADS) k_bp(BpArgs p)
                     if constexpr (GRP) {
                         bp_store1_grp<VT>(p, blockIdx.z, q, ys0 + q, Z, X, sum[j][i], cnt[j][i]);
                     } else {
-                        const float nv = bp_store<MODE>(p, ys0 + q, Z, X, sum[j][i], cnt[j][i]);
+                        const float k = cnt[j][i] > 0 ? __fdiv_rn(MODE == 0 ? p.relax : 1.f, (float)cnt[j][i]) : 0.f;
+                        const float nv = bp_store<MODE>(p, ys0 + q, Z, X, sum[j][i], cnt[j][i], k);
                         if constexpr (MODE == 0 && !std::is_same<VT, float>::value) shadow_one<VT>(p, ys0 + q, Z, X, nv);
                     }
                 }
@@ -761,18 +782,25 @@ __global__ void __launch_bounds__(256) k_fp_diff(const float* __restrict__ vol, 
                                                         : reinterpret_cast<const T4*>(shadow)) +
                        (size_t)blockIdx.z * slice + (size_t)(Nz - 1) * Nx;
         const T4* g1 = g0 - Nx;
-        for (int i = wlo; i <= whi; i++) {
+        // cell offset iX - iZ*Nx from the bits of x + 2^23 and z + 2^23
+        // (wrapping 32-bit arithmetic; the true value fits an int)
+        const unsigned kx = (unsigned)kMagicBits * (unsigned)(Nx - 1);
+        float fi = (float)wlo;   // i as a float, exact below 2^24
+        for (int i = wlo; i <= whi; i++, fi += 1.f) {
             if (i < lo || i > hi) continue;
-            const float fX = r.x(i), fZ = r.z(i);
-            const int iX = (int)fX, iZ = (int)fZ;
-            const float wx = fX - (float)iX, wz = fZ - (float)iZ;
-            const int o = iX - iZ * Nx;
+            const float fd = fi - r.halfL;   // exact: the sample index of RayPos
+            const float fX = __fmaf_rn(-fd, r.s, r.tx), fZ = __fmaf_rn(fd, r.c, r.tz);
+            const float tX = __fadd_rd(fX, kMagic), tZ = __fadd_rd(fZ, kMagic);
+            const float wx = fX - (tX - kMagic), wz = fZ - (tZ - kMagic);
+            const int o = (int)((unsigned)__float_as_int(tX) - (unsigned)__float_as_int(tZ) * (unsigned)Nx + kx);
+            const float ux = 1.f - wx, uz = 1.f - wz;
+            const float w00 = ux * uz, w10 = wx * uz, w01 = ux * wz, w11 = wx * wz;
             const float4 a00 = Quad<VT>::ld(g0 + o), a10 = Quad<VT>::ld(g0 + o + 1);
             const float4 a01 = Quad<VT>::ld(g1 + o), a11 = Quad<VT>::ld(g1 + o + 1);
-            fSum[0] += bilerp(a00.x, a10.x, a01.x, a11.x, wx, wz);
-            fSum[1] += bilerp(a00.y, a10.y, a01.y, a11.y, wx, wz);
-            fSum[2] += bilerp(a00.z, a10.z, a01.z, a11.z, wx, wz);
-            fSum[3] += bilerp(a00.w, a10.w, a01.w, a11.w, wx, wz);
+            fSum[0] = __fmaf_rn(w11, a11.x, __fmaf_rn(w01, a01.x, __fmaf_rn(w10, a10.x, __fmaf_rn(w00, a00.x, fSum[0]))));
+            fSum[1] = __fmaf_rn(w11, a11.y, __fmaf_rn(w01, a01.y, __fmaf_rn(w10, a10.y, __fmaf_rn(w00, a00.y, fSum[1]))));
+            fSum[2] = __fmaf_rn(w11, a11.z, __fmaf_rn(w01, a01.z, __fmaf_rn(w10, a10.z, __fmaf_rn(w00, a00.z, fSum[2]))));
+            fSum[3] = __fmaf_rn(w11, a11.w, __fmaf_rn(w01, a01.w, __fmaf_rn(w10, a10.w, __fmaf_rn(w00, a00.w, fSum[3]))));
         }
         const float n = (float)max(hi - lo + 1, 0);
 #pragma unroll
