@@ -93,6 +93,17 @@ void host_fft_pow2(std::vector<std::complex<double>>& a, int sign)
 
 at3r_status dalloc_bytes(at3r_plan* p, void** ptr, size_t bytes);   // defined with the plan
 
+// Per-stage divisors of the Stockham index arithmetic.
+void set_stage_divs(FftDirect& d)
+{
+    int ns = 1;
+    for (int i = 0; i < d.nst; i++) {
+        d.by_nb[i] = make_fast_div((unsigned)(d.n / d.radix[i]));
+        d.by_ns[i] = make_fast_div((unsigned)ns);
+        ns *= d.radix[i];
+    }
+}
+
 at3r_status make_fft(at3r_plan* pl, int n, HostFft& h)
 {
     std::vector<int> rad;
@@ -105,6 +116,7 @@ at3r_status make_fft(at3r_plan* pl, int n, HostFft& h)
         p.d.n = n;
         p.d.nst = (n == 1) ? 0 : (int)rad.size();
         for (int i = 0; i < p.d.nst; i++) p.d.radix[i] = rad[i];
+        set_stage_divs(p.d);
         fill_twiddles(tw, n);
     } else {
         int m = 1;
@@ -115,6 +127,7 @@ at3r_status make_fft(at3r_plan* pl, int n, HostFft& h)
         p.d.n = m;
         p.d.nst = (int)rad.size();
         for (int i = 0; i < p.d.nst; i++) p.d.radix[i] = rad[i];
+        set_stage_divs(p.d);
         fill_twiddles(tw, m);
         chirp.resize(n);
         std::vector<std::complex<double>> cd(n);
@@ -245,6 +258,7 @@ struct at3r_plan {
     float2* d_y = nullptr;
     HostFft fN, f2x, f2z, fz, fx;
     int zcrop_cb = 4, zcrop_pitch = 0;
+    int b_rweight = 1, b_row = 1, b_xc2r = 1;   // sequences per CTA of the row FFT kernels
     size_t smem_rweight = 0, smem_row = 0, smem_zcrop = 0, smem_xc2r = 0;
     int bp_ww_sart = 0, bp_ww_wbp = 0;
     // host path
@@ -444,9 +458,9 @@ at3r_status run_slab_t(at3r_plan* p, const float* proj, size_t tilt_stride, int 
     }
     // WBP
     TB(p, st);
-    k_rweight<ST><<<dim3((T + 1) / 2, S), 512, p->smem_rweight, st>>>(proj, tilt_stride, p->nx, proj_y0, p->d_cs, T,
-                                                                      N, Nz, p->d_h, p->fN.plan, filt, p->d_scale,
-                                                                      p->d_flags);
+    k_rweight<ST><<<dim3(((T + 1) / 2 + p->b_rweight - 1) / p->b_rweight, S), 512, p->smem_rweight, st>>>(
+        proj, tilt_stride, p->nx, proj_y0, p->d_cs, T, N, Nz, p->d_h, p->fN.plan, p->b_rweight, filt, p->d_scale,
+        p->d_flags);
     TE(p, st, KK_RWEIGHT, (f4 + es) * S * T * N, (double)S * T * N);
     BpArgs a{};
     a.sino = filt; a.scale = p->d_scale; a.shadow = nullptr; a.T = T; a.N = N; a.t0 = 0; a.t1 = T; a.cs = p->d_cs;
@@ -457,7 +471,8 @@ at3r_status run_slab_t(at3r_plan* p, const float* proj, size_t tilt_stride, int 
     k_bp<1, ST, float, false><<<bgrid, BP_THREADS, bp_smem(T, a.ww), st>>>(a);
     TE(p, st, KK_BP_WBP, es * S * (double)T * N + f4 * 4 * vox, 4 * vox * T);
     TB(p, st);
-    k_row_r2c<<<dim3(Nz, S), 512, p->smem_row, st>>>(p->d_g2, Nx, Nz, p->f2x.plan, p->d_y);
+    k_row_r2c<<<dim3((Nz + p->b_row - 1) / p->b_row, S), 512, p->smem_row, st>>>(p->d_g2, Nx, Nz, p->f2x.plan,
+                                                                                   p->b_row, p->d_y);
     TE(p, st, KK_ROW_R2C, f4 * 4 * vox + 8.0 * S * 2 * Nz * KX, 4 * vox);
     const float norm = (float)(1.0 / (2.0 * Nx) / (2.0 * Nz));
     float2* w = reinterpret_cast<float2*>(p->d_g2);
@@ -466,7 +481,8 @@ at3r_status run_slab_t(at3r_plan* p, const float* proj, size_t tilt_stride, int 
         p->d_y, Nx, Nz, p->zcrop_cb, p->zcrop_pitch, p->f2z.plan, p->fz.plan, norm, w);
     TE(p, st, KK_ZCROP, 8.0 * S * 3 * Nz * KX, (double)S * 2 * Nz * KX);
     TB(p, st);
-    k_x_c2r<<<dim3((Nz + 1) / 2, S), 512, p->smem_xc2r, st>>>(w, Nx, Nz, p->fx.plan, p->c2r == AT3R_C2R_PACKED, vol,
+    k_x_c2r<<<dim3(((Nz + 1) / 2 + p->b_xc2r - 1) / p->b_xc2r, S), 512, p->smem_xc2r, st>>>(
+        w, Nx, Nz, p->fx.plan, p->b_xc2r, p->c2r == AT3R_C2R_PACKED, vol,
                                                               (size_t)Nx * Nz);
     TE(p, st, KK_XC2R, 8.0 * S * Nz * KX + f4 * vox, vox);
     return AT3R_OK;
@@ -630,11 +646,22 @@ at3r_status plan_create_impl(const at3r_geom* g, cudaStream_t alloc_stream, at3r
         if ((rc = make_fft(p, 2 * p->Nz, p->f2z))) return fail(rc);
         if ((rc = make_fft(p, p->Nz, p->fz))) return fail(rc);
         if ((rc = make_fft(p, p->Nx, p->fx))) return fail(rc);
-        p->smem_rweight = 2 * sizeof(float2) * p->fN.plan.work;
-        p->smem_row = 2 * sizeof(float2) * p->f2x.plan.work;
-        p->smem_xc2r = 2 * sizeof(float2) * p->fx.plan.work;
+        // sequences per CTA: enough butterflies per stage for 512 threads,
+        // two buffers of them within 96 KB (two CTAs per SM) where possible
+        auto batch = [](int work) {
+            int b = 1;
+            while (b < 8 && (size_t)work * b * 2 <= 4096) b *= 2;
+            while (b > 1 && 2 * sizeof(float2) * (size_t)work * b > (96u << 10)) b /= 2;
+            return b;
+        };
+        p->b_rweight = batch(p->fN.plan.work);
+        p->b_row = batch(p->f2x.plan.work);
+        p->b_xc2r = batch(p->fx.plan.work);
+        p->smem_rweight = 2 * sizeof(float2) * p->fN.plan.work * p->b_rweight;
+        p->smem_row = 2 * sizeof(float2) * p->f2x.plan.work * p->b_row;
+        p->smem_xc2r = 2 * sizeof(float2) * p->fx.plan.work * p->b_xc2r;
         p->zcrop_pitch = round_up(std::max(p->f2z.plan.work, p->fz.plan.work), 2) + 1;
-        p->zcrop_cb = 4;
+        p->zcrop_cb = std::max(4, std::min(32, 4096 / (2 * p->Nz)));
         while (p->zcrop_cb > 1 && 2 * sizeof(float2) * p->zcrop_cb * p->zcrop_pitch > 227 * 1024) p->zcrop_cb /= 2;
         p->smem_zcrop = 2 * sizeof(float2) * p->zcrop_cb * p->zcrop_pitch;
         p->bp_ww_wbp = bp_window(BP_TX, BP_TZ, 0.5, cs, p->T);

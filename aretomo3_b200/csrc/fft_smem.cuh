@@ -18,10 +18,36 @@ namespace at3r {
 
 constexpr int kMaxFftStages = 32;
 
+// Division by a stage constant d as a multiply and shift: for x < 2^24,
+// floor(x / d) = (x * m) >> (24 + l) with l = ceil(log2 d), m = ceil(2^(24+l) / d)
+// (the error x (m d - 2^(24+l)) / (d 2^(24+l)) stays below 2^-l <= 1/d); on
+// the device (x * m) >> 24 is the high word of (x << 8) * m.
+struct FastDiv {
+    unsigned m;
+    int l;
+};
+__host__ __device__ inline unsigned fast_div(unsigned x, FastDiv d)
+{
+#ifdef __CUDA_ARCH__
+    return __umulhi(x << 8, d.m) >> d.l;
+#else
+    return (unsigned)(((unsigned long long)x * d.m) >> (24 + d.l));
+#endif
+}
+inline FastDiv make_fast_div(unsigned d)
+{
+    int l = 0;
+    while ((1u << l) < d) l++;
+    const unsigned long long p = 1ull << (24 + l);
+    return FastDiv{(unsigned)((p + d - 1) / d), l};
+}
+
 struct FftDirect {
     int n;                       // length
     int nst;                     // number of stages
     int radix[kMaxFftStages];    // radix of each stage (product = n)
+    FastDiv by_nb[kMaxFftStages];   // division by n / radix[s]
+    FastDiv by_ns[kMaxFftStages];   // division by the product of the radices before stage s
     const float2* tw;            // exp(-2 pi i k / n), k in [0, n)
 };
 
@@ -171,17 +197,19 @@ template <> struct Dft<13> : DftGeneric<13> {};
 // with pitch `pitch` (complex elements).
 template <int R>
 __device__ __forceinline__ void stockham_stage(const float2* __restrict__ in, float2* __restrict__ out,
-                                               const FftDirect& d, int Ns, int batch, int pitch, int sign)
+                                               const FftDirect& d, int st, int Ns, int batch, int pitch, int sign)
 {
     const int nb = d.n / R;
     const int total = nb * batch;
     const int twbase = d.n / (Ns * R);
+    const FastDiv dnb = d.by_nb[st], dns = d.by_ns[st];
     for (int idx = threadIdx.x; idx < total; idx += blockDim.x) {
-        const int q = idx / nb;
+        const int q = (int)fast_div((unsigned)idx, dnb);
         const int j = idx - q * nb;
         const float2* src = in + (size_t)q * pitch;
         float2* dst = out + (size_t)q * pitch;
-        const int jm = j % Ns;
+        const int jq = (int)fast_div((unsigned)j, dns);
+        const int jm = j - jq * Ns;
         float2 v[R];
 #pragma unroll
         for (int r = 0; r < R; r++) v[r] = src[j + r * nb];
@@ -191,7 +219,7 @@ __device__ __forceinline__ void stockham_stage(const float2* __restrict__ in, fl
             for (int r = 1; r < R; r++) v[r] = cmul(v[r], twiddle(d.tw, r * ts, sign));
         }
         Dft<R>::run(v, sign, d.tw, d.n);
-        const int od = (j / Ns) * Ns * R + jm;
+        const int od = jq * Ns * R + jm;
 #pragma unroll
         for (int r = 0; r < R; r++) dst[od + r * Ns] = v[r];
     }
@@ -205,14 +233,14 @@ __device__ inline float2* stockham(float2* a, float2* b, const FftDirect& d, int
     for (int s = 0; s < d.nst; s++) {
         const int R = d.radix[s];
         switch (R) {
-            case 2: stockham_stage<2>(a, b, d, Ns, batch, pitch, sign); break;
-            case 3: stockham_stage<3>(a, b, d, Ns, batch, pitch, sign); break;
-            case 4: stockham_stage<4>(a, b, d, Ns, batch, pitch, sign); break;
-            case 5: stockham_stage<5>(a, b, d, Ns, batch, pitch, sign); break;
-            case 7: stockham_stage<7>(a, b, d, Ns, batch, pitch, sign); break;
-            case 8: stockham_stage<8>(a, b, d, Ns, batch, pitch, sign); break;
-            case 11: stockham_stage<11>(a, b, d, Ns, batch, pitch, sign); break;
-            case 13: stockham_stage<13>(a, b, d, Ns, batch, pitch, sign); break;
+            case 2: stockham_stage<2>(a, b, d, s, Ns, batch, pitch, sign); break;
+            case 3: stockham_stage<3>(a, b, d, s, Ns, batch, pitch, sign); break;
+            case 4: stockham_stage<4>(a, b, d, s, Ns, batch, pitch, sign); break;
+            case 5: stockham_stage<5>(a, b, d, s, Ns, batch, pitch, sign); break;
+            case 7: stockham_stage<7>(a, b, d, s, Ns, batch, pitch, sign); break;
+            case 8: stockham_stage<8>(a, b, d, s, Ns, batch, pitch, sign); break;
+            case 11: stockham_stage<11>(a, b, d, s, Ns, batch, pitch, sign); break;
+            case 13: stockham_stage<13>(a, b, d, s, Ns, batch, pitch, sign); break;
             default: break;  // host planning never emits another radix
         }
         __syncthreads();

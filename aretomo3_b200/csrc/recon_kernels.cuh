@@ -214,61 +214,85 @@ __global__ void __launch_bounds__(256) k_gather_weight(const float* __restrict__
 // imaginary parts of one complex sequence: the filter H(k) is real and even
 // (H(N-k) = H(k)), so filtering a + ib filters a and b independently.
 // AreTomo/Recon/GWeightProjs.cu:18, GRWeight.cu:7-23 (+ MaUtil/GFFT1D.cu R2C/C2R).
-// Grid (ceil(T/2), slices).
+// B such pairs per CTA, transformed as one batch (B <= 8: one warp per row
+// for the 16-bit row scales).  Grid (ceil(ceil(T/2) / B), slices).
 // ---------------------------------------------------------------------------
 template <typename ST>
 __global__ void __launch_bounds__(512) k_rweight(const float* __restrict__ proj, size_t tilt_stride, int row_pitch,
                                                  int y0, const float2* __restrict__ cs, int T, int N, int Nz,
-                                                 const float* __restrict__ hhalf, FftPlan plan, ST* __restrict__ out,
-                                                 float* __restrict__ scale, int* __restrict__ flags)
+                                                 const float* __restrict__ hhalf, const __grid_constant__ FftPlan plan, int B,
+                                                 ST* __restrict__ out, float* __restrict__ scale,
+                                                 int* __restrict__ flags)
 {
     extern __shared__ float2 fsm[];
+    __shared__ float rsc[16];   // per row of the CTA: 1 / scale
+    const int pitch = plan.work;
     float2* a = fsm;
-    float2* b = fsm + plan.work;
-    const int t0 = 2 * blockIdx.x, t1 = t0 + 1, ys = blockIdx.y;
-    const bool two = t1 < T;
-    const float w0 = __ldg(&cs[t0].x) / (float)Nz;
-    const float w1 = two ? __ldg(&cs[t1].x) / (float)Nz : 0.f;
-    const float* s0 = proj + (size_t)t0 * tilt_stride + (size_t)(y0 + ys) * row_pitch;
-    const float* s1 = proj + (size_t)(two ? t1 : t0) * tilt_stride + (size_t)(y0 + ys) * row_pitch;
-    for (int x = threadIdx.x; x < N; x += blockDim.x)
-        a[x] = make_float2(__ldg(s0 + x) * w0, two ? __ldg(s1 + x) * w1 : 0.f);
-    __syncthreads();
-    float2* r = fft_run(a, b, plan, 1, plan.work, -1);
-    for (int k = threadIdx.x; k < N; k += blockDim.x) {
-        const float h = __ldg(hhalf + (k <= N - k ? k : N - k));
-        float2 v = r[k];
-        r[k] = make_float2(v.x * h, v.y * h);
+    float2* b = fsm + (size_t)B * pitch;
+    const int ys = blockIdx.y, pair0 = blockIdx.x * B;
+    const int nq = min(B, (T + 1) / 2 - pair0);   // tilt pairs in this CTA
+    const float* srow = proj + (size_t)(y0 + ys) * row_pitch;
+    for (int q = 0; q < nq; q++) {
+        const int t0 = 2 * (pair0 + q), t1 = t0 + 1;
+        const bool two = t1 < T;
+        const float w0 = __ldg(&cs[t0].x) / (float)Nz;
+        const float w1 = two ? __ldg(&cs[t1].x) / (float)Nz : 0.f;
+        const float* s0 = srow + (size_t)t0 * tilt_stride;
+        const float* s1 = srow + (size_t)(two ? t1 : t0) * tilt_stride;
+        float2* aq = a + (size_t)q * pitch;
+        for (int x = threadIdx.x; x < N; x += blockDim.x)
+            aq[x] = make_float2(__ldg(s0 + x) * w0, two ? __ldg(s1 + x) * w1 : 0.f);
     }
     __syncthreads();
-    float2* r2 = fft_run(r, r == a ? b : a, plan, 1, plan.work, +1);
-    ST* d0 = out + ((size_t)ys * T + t0) * N;
-    float inv0 = 1.f, inv1 = 1.f;
+    float2* r = fft_run(a, b, plan, nq, pitch, -1);
+    for (int q = 0; q < nq; q++) {
+        float2* rq = r + (size_t)q * pitch;
+        for (int k = threadIdx.x; k < N; k += blockDim.x) {
+            const float h = __ldg(hhalf + (k <= N - k ? k : N - k));
+            const float2 v = rq[k];
+            rq[k] = make_float2(v.x * h, v.y * h);
+        }
+    }
+    __syncthreads();
+    float2* r2 = fft_run(r, r == a ? b : a, plan, nq, pitch, +1);
+    // row 2q + c of the CTA is tilt 2(pair0 + q) + c, component c of sequence q
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     if constexpr (!std::is_same<ST, float>::value) {
-        __shared__ float red[32];
-        float m0 = 0.f, m1 = 0.f;
-        for (int x = threadIdx.x; x < N; x += blockDim.x) {
-            const float2 v = r2[x];
-            if (v.x > kSentinelTest) m0 = fmaxf(m0, fabsf(v.x));
-            if (v.y > kSentinelTest) m1 = fmaxf(m1, fabsf(v.y));
+        // one warp per row: the row's largest non-empty magnitude is its scale
+        if (warp < 2 * nq) {
+            const int q = warp >> 1, c = warp & 1, t = 2 * (pair0 + q) + c;
+            const float2* rq = r2 + (size_t)q * pitch;
+            float m = 0.f;
+            for (int x = lane; x < N; x += 32) {
+                const float v = c ? rq[x].y : rq[x].x;
+                if (v > kSentinelTest) m = fmaxf(m, fabsf(v));
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+            const float sc = row_scale(m);
+            if (lane == 0) {
+                rsc[warp] = 1.f / sc;
+                if (t < T) scale[(size_t)ys * T + t] = sc;
+            }
         }
-        const float s0 = row_scale(block_absmax(m0, red));
-        const float s1 = row_scale(block_absmax(m1, red));
-        inv0 = 1.f / s0;
-        inv1 = 1.f / s1;
-        if (threadIdx.x == 0) {
-            scale[(size_t)ys * T + t0] = s0;
-            if (two) scale[(size_t)ys * T + t0 + 1] = s1;
-        }
+        __syncthreads();
     }
     bool low = false;
-    for (int x = threadIdx.x; x < N; x += blockDim.x) {
-        const float2 v = r2[x];
-        Stor<ST>::st(d0 + x, v.x, inv0);
-        low |= v.x <= kLowValue;
-        if (two) {
-            Stor<ST>::st(d0 + N + x, v.y, inv1);
-            low |= v.y <= kLowValue;
+    for (int q = 0; q < nq; q++) {
+        const int t0 = 2 * (pair0 + q);
+        const bool two = t0 + 1 < T;
+        const float2* rq = r2 + (size_t)q * pitch;
+        ST* d0 = out + ((size_t)ys * T + t0) * N;
+        const float inv0 = std::is_same<ST, float>::value ? 1.f : rsc[2 * q];
+        const float inv1 = std::is_same<ST, float>::value ? 1.f : rsc[2 * q + 1];
+        for (int x = threadIdx.x; x < N; x += blockDim.x) {
+            const float2 v = rq[x];
+            Stor<ST>::st(d0 + x, v.x, inv0);
+            low |= v.x <= kLowValue;
+            if (two) {
+                Stor<ST>::st(d0 + N + x, v.y, inv1);
+                low |= v.y <= kLowValue;
+            }
         }
     }
     if (low) atomicOr(flags + ys, kFlagRawLow);
@@ -982,26 +1006,34 @@ __global__ void __launch_bounds__(256) k_fill_empty(float* __restrict__ vol, siz
 // bins kx in [0, Nx/2].  Two rows per CTA as one complex sequence z = a + ib:
 // A[k] = (Z[k] + conj Z[-k]) / 2, B[k] = (Z[k] - conj Z[-k]) / 2i.
 // g: [slices][2Nz][2Nx]; y: [slices][2Nz][KX] with KX = Nx/2 + 1.
-// Grid (Nz, slices): CTA r handles rows 2r, 2r+1.
+// B row pairs per CTA.  Grid (ceil(Nz / B), slices).
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(512) k_row_r2c(const float* __restrict__ g, int Nx, int Nz, FftPlan plan,
+__global__ void __launch_bounds__(512) k_row_r2c(const float* __restrict__ g, int Nx, int Nz, const __grid_constant__ FftPlan plan, int B,
                                                  float2* __restrict__ y)
 {
     extern __shared__ float2 fsm[];
+    const int pitch = plan.work;
     float2* a = fsm;
-    float2* b = fsm + plan.work;
+    float2* b = fsm + (size_t)B * pitch;
     const int X2 = 2 * Nx, KX = Nx / 2 + 1;
-    const int r0 = 2 * blockIdx.x, ys = blockIdx.y;
-    const float* g0 = g + ((size_t)ys * 2 * Nz + r0) * X2;
-    for (int x = threadIdx.x; x < X2; x += blockDim.x) a[x] = make_float2(__ldg(g0 + x), __ldg(g0 + X2 + x));
+    const int pr0 = blockIdx.x * B, ys = blockIdx.y;   // row pairs (2 pr, 2 pr + 1) of the 2Nz rows
+    const int nq = min(B, Nz - pr0);
+    for (int q = 0; q < nq; q++) {
+        const float* g0 = g + ((size_t)ys * 2 * Nz + 2 * (pr0 + q)) * X2;
+        float2* aq = a + (size_t)q * pitch;
+        for (int x = threadIdx.x; x < X2; x += blockDim.x) aq[x] = make_float2(__ldg(g0 + x), __ldg(g0 + X2 + x));
+    }
     __syncthreads();
-    const float2* Z = fft_run(a, b, plan, 1, plan.work, -1);
-    float2* y0 = y + ((size_t)ys * 2 * Nz + r0) * KX;
-    for (int k = threadIdx.x; k < KX; k += blockDim.x) {
-        const float2 p = Z[k], q = Z[k == 0 ? 0 : X2 - k];
-        // A = (p + conj q)/2 ; B = (p - conj q)/(2i) = -i (p - conj q)/2
-        y0[k] = make_float2(0.5f * (p.x + q.x), 0.5f * (p.y - q.y));
-        y0[KX + k] = make_float2(0.5f * (p.y + q.y), -0.5f * (p.x - q.x));
+    const float2* Zs = fft_run(a, b, plan, nq, pitch, -1);
+    for (int q = 0; q < nq; q++) {
+        const float2* Z = Zs + (size_t)q * pitch;
+        float2* y0 = y + ((size_t)ys * 2 * Nz + 2 * (pr0 + q)) * KX;
+        for (int k = threadIdx.x; k < KX; k += blockDim.x) {
+            const float2 p = Z[k], qv = Z[k == 0 ? 0 : X2 - k];
+            // A = (p + conj q)/2 ; B = (p - conj q)/(2i) = -i (p - conj q)/2
+            y0[k] = make_float2(0.5f * (p.x + qv.x), 0.5f * (p.y - qv.y));
+            y0[KX + k] = make_float2(0.5f * (p.y + qv.y), -0.5f * (p.x - qv.x));
+        }
     }
 }
 
@@ -1014,7 +1046,7 @@ __global__ void __launch_bounds__(512) k_row_r2c(const float* __restrict__ g, in
 // y: [slices][2Nz][KX] -> w: [slices][Nz][KX].  Grid (ceil(KX/CB), slices).
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(512) k_zcrop(const float2* __restrict__ y, int Nx, int Nz, int CB, int pitch,
-                                               FftPlan p2, FftPlan p1, float norm, float2* __restrict__ w)
+                                               const __grid_constant__ FftPlan p2, const __grid_constant__ FftPlan p1, float norm, float2* __restrict__ w)
 {
     extern __shared__ float2 fsm[];
     const int KX = Nx / 2 + 1, Z2 = 2 * Nz;
@@ -1053,41 +1085,55 @@ __global__ void __launch_bounds__(512) k_zcrop(const float2* __restrict__ y, int
 // Hermitian-wise inverts to a + ib.  packed != 0 then adds what cuFFT's
 // half-length packing algorithm makes of those imaginary parts:
 // -(Im A0 + Im A_{Nx/2}) on even and (Im A0 - Im A_{Nx/2}) on odd samples.
-// w: [slices][Nz][KX] -> vol: [slices][Nz][Nx] (row Nz-1-z).  Grid (ceil(Nz/2), slices).
+// w: [slices][Nz][KX] -> vol: [slices][Nz][Nx] (row Nz-1-z).  B row pairs per
+// CTA.  Grid (ceil(ceil(Nz/2) / B), slices).
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(512) k_x_c2r(const float2* __restrict__ w, int Nx, int Nz, FftPlan plan,
+__global__ void __launch_bounds__(512) k_x_c2r(const float2* __restrict__ w, int Nx, int Nz, const __grid_constant__ FftPlan plan, int B,
                                                int packed, float* __restrict__ vol, size_t vol_slice)
 {
     extern __shared__ float2 fsm[];
+    const int pitch = plan.work;
     float2* a = fsm;
-    float2* b = fsm + plan.work;
+    float2* b = fsm + (size_t)B * pitch;
     const int KX = Nx / 2 + 1, H = Nx / 2;
-    const int z0 = 2 * blockIdx.x, z1 = z0 + 1, ys = blockIdx.y;
-    const bool two = z1 < Nz;
-    const float2* A = w + ((size_t)ys * Nz + z0) * KX;
-    const float2* B = A + KX;
-    for (int k = threadIdx.x; k < Nx; k += blockDim.x) {
-        const bool lo = k <= H;
-        const int kk = lo ? k : Nx - k;
-        float2 av = A[kk];
-        float2 bv = two ? B[kk] : make_float2(0.f, 0.f);
-        if (kk == 0 || kk == H) { av.y = 0.f; bv.y = 0.f; }
-        if (!lo) { av.y = -av.y; bv.y = -bv.y; }
-        a[k] = make_float2(av.x - bv.y, av.y + bv.x);   // A + iB
+    const int pz0 = blockIdx.x * B, ys = blockIdx.y;   // z pairs (2 pz, 2 pz + 1)
+    const int nq = min(B, (Nz + 1) / 2 - pz0);
+    for (int q = 0; q < nq; q++) {
+        const int z0 = 2 * (pz0 + q);
+        const bool two = z0 + 1 < Nz;
+        const float2* A = w + ((size_t)ys * Nz + z0) * KX;
+        const float2* Bv = A + KX;
+        float2* aq = a + (size_t)q * pitch;
+        for (int k = threadIdx.x; k < Nx; k += blockDim.x) {
+            const bool lo = k <= H;
+            const int kk = lo ? k : Nx - k;
+            float2 av = A[kk];
+            float2 bv = two ? Bv[kk] : make_float2(0.f, 0.f);
+            if (kk == 0 || kk == H) { av.y = 0.f; bv.y = 0.f; }
+            if (!lo) { av.y = -av.y; bv.y = -bv.y; }
+            aq[k] = make_float2(av.x - bv.y, av.y + bv.x);   // A + iB
+        }
     }
     __syncthreads();
-    const float2* r = fft_run(a, b, plan, 1, plan.work, +1);
-    float ea = 0.f, oa = 0.f, eb = 0.f, ob = 0.f;
-    if (packed) {
-        const float ia0 = A[0].y, iah = A[H].y;
-        ea = -(ia0 + iah); oa = ia0 - iah;
-        if (two) { const float ib0 = B[0].y, ibh = B[H].y; eb = -(ib0 + ibh); ob = ib0 - ibh; }
-    }
-    float* o0 = vol + (size_t)ys * vol_slice + (size_t)(Nz - 1 - z0) * Nx;
-    for (int x = threadIdx.x; x < Nx; x += blockDim.x) {
-        const float2 v = r[x];
-        o0[x] = v.x + ((x & 1) ? oa : ea);
-        if (two) o0[x - Nx] = v.y + ((x & 1) ? ob : eb);
+    const float2* rs = fft_run(a, b, plan, nq, pitch, +1);
+    for (int q = 0; q < nq; q++) {
+        const int z0 = 2 * (pz0 + q);
+        const bool two = z0 + 1 < Nz;
+        const float2* A = w + ((size_t)ys * Nz + z0) * KX;
+        const float2* Bv = A + KX;
+        const float2* r = rs + (size_t)q * pitch;
+        float ea = 0.f, oa = 0.f, eb = 0.f, ob = 0.f;
+        if (packed) {
+            const float ia0 = A[0].y, iah = A[H].y;
+            ea = -(ia0 + iah); oa = ia0 - iah;
+            if (two) { const float ib0 = Bv[0].y, ibh = Bv[H].y; eb = -(ib0 + ibh); ob = ib0 - ibh; }
+        }
+        float* o0 = vol + (size_t)ys * vol_slice + (size_t)(Nz - 1 - z0) * Nx;
+        for (int x = threadIdx.x; x < Nx; x += blockDim.x) {
+            const float2 v = r[x];
+            o0[x] = v.x + ((x & 1) ? oa : ea);
+            if (two) o0[x - Nx] = v.y + ((x & 1) ? ob : eb);
+        }
     }
 }
 
