@@ -14,33 +14,11 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include "fast_div.h"
+
 namespace at3r {
 
 constexpr int kMaxFftStages = 32;
-
-// Division by a stage constant d as a multiply and shift: for x < 2^24,
-// floor(x / d) = (x * m) >> (24 + l) with l = ceil(log2 d), m = ceil(2^(24+l) / d)
-// (the error x (m d - 2^(24+l)) / (d 2^(24+l)) stays below 2^-l <= 1/d); on
-// the device (x * m) >> 24 is the high word of (x << 8) * m.
-struct FastDiv {
-    unsigned m;
-    int l;
-};
-__host__ __device__ inline unsigned fast_div(unsigned x, FastDiv d)
-{
-#ifdef __CUDA_ARCH__
-    return __umulhi(x << 8, d.m) >> d.l;
-#else
-    return (unsigned)(((unsigned long long)x * d.m) >> (24 + d.l));
-#endif
-}
-inline FastDiv make_fast_div(unsigned d)
-{
-    int l = 0;
-    while ((1u << l) < d) l++;
-    const unsigned long long p = 1ull << (24 + l);
-    return FastDiv{(unsigned)((p + d - 1) / d), l};
-}
 
 struct FftDirect {
     int n;                       // length

@@ -88,10 +88,11 @@ STORAGE = {"f32": 0, "f16": 1, "bf16": 2}
 def plan_kwargs(c) -> dict:
     from aretomo3_b200 import recon
     st = STORAGE[c.get("storage", "f32")]
+    slab = int(c.get("slab", 0))
     if c["method"] == "sart":
         return dict(method=recon.SART, start_tilt=0, num_tilts=len(c["tilts"]), iterations=c["iters"],
-                    subsets=c["subsets"], relax=c.get("relax", 0.0), storage=st)
-    return dict(method=recon.WBP, storage=st)
+                    subsets=c["subsets"], relax=c.get("relax", 0.0), storage=st, slab_slices=slab)
+    return dict(method=recon.WBP, storage=st, slab_slices=slab)
 
 
 # --- clocks -----------------------------------------------------------------
@@ -152,13 +153,40 @@ def measured_peaks() -> dict:
     return {"hbm_gbs": 6650.0, "source": "fallback"}
 
 
-def profiled_traffic(kernel: str, workload_name: str):
+def profiled_traffic(kernel: str, workload_name: str, storage: str):
     """DRAM bytes per launch of `kernel` from the committed ncu summary, if any."""
     p = os.path.join(ROOT, "profiles", "traffic.json")
     if not os.path.exists(p):
         return None
     d = json.load(open(p))
-    return d.get(workload_name, {}).get(kernel)
+    return d.get(f"{workload_name}/{storage}", {}).get(kernel)
+
+
+# Shared-memory / L1 bytes one work unit of a kernel moves on chip: the back-
+# projectors read one 8-byte (p[i], p[i+1]) pair per voxel, tilt and slice;
+# the forward projector reads four bilinear taps per ray sample and slice (a
+# 16-byte load serves four slices: 16 B per sample-slice, 8 B from the 16-bit
+# shadow).
+def onchip_bytes_per_unit(kernel: str, storage: str):
+    if kernel in ("bp_sart", "bp_wbp_2x"):
+        return 8.0
+    if kernel == "fp_diff":
+        return 16.0 if storage == "f32" else 8.0
+    return None
+
+
+def onchip_roof(kernel: str, d: dict, storage: str, clk: dict):
+    """The kernel's algorithmic L1/shared-memory bytes per second against the
+    data path's 128 B/clk/SM over 148 SMs at the SM clock sampled during the
+    timed region."""
+    b = onchip_bytes_per_unit(kernel, storage)
+    mhz = clk.get("sm_mhz") or 1965.0
+    if b is None or not d["ms"]:
+        return None
+    achieved = b * d["units"] / (d["ms"] / 1e3) / 1e12
+    peak = 148 * 128 * mhz * 1e6 / 1e12
+    return {"resource": "L1/shared-memory data path", "bytes_per_unit": b, "achieved": achieved, "peak": peak,
+            "unit": "TB/s", "frac": achieved / peak, "sm_mhz": mhz}
 
 
 # --- CPU side (oracle/ FP32 port): baseline leg and reference arm ------------
@@ -195,9 +223,10 @@ def cpu_baseline(c, frames, threads) -> dict:
                       f"{dt:.2f} s"}
 
 
-def error_vs_oracle(c, frames, vol_gpu, n_slices=2) -> dict:
+def error_vs_oracle(c, frames, vol_gpu, n_slices=2, mid=None) -> dict:
     """Relative L2 / max-abs of the GPU volume against the FP64 oracle on a few
-    slices (the checker)."""
+    slices (the checker).  `mid`: those slices alone, when the whole volume was
+    not copied back."""
     ol = _oracle()
     y0 = c["ny"] // 2
     if c["method"] == "sart":
@@ -207,7 +236,7 @@ def error_vs_oracle(c, frames, vol_gpu, n_slices=2) -> dict:
         from aretomo3_b200 import recon
         mode = 1 if c.get("_c2r") == recon.C2R_PACKED else 0
         ref = ol.wbp(frames, c["tilts"], c["vol_z"], y0=y0, y1=y0 + n_slices, c2r_mode=mode)
-    got = vol_gpu[y0:y0 + n_slices].astype(np.float64)
+    got = (mid if mid is not None else vol_gpu[y0:y0 + n_slices]).astype(np.float64)
     return {"rel_l2": float(np.linalg.norm(got - ref) / np.linalg.norm(ref)),
             "max_abs": float(np.abs(got - ref).max()), "slices": n_slices, "against": "FP64 oracle"}
 
@@ -291,22 +320,36 @@ def run_our_arm(args, c, rank, world, local_rank):
     launches_per_step = plan.last_launches
     plan.set_timing(False)
 
-    # same steps without per-launch events (overhead of the instrumentation)
-    torch.cuda.synchronize()
-    f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    f0.record(stream)
-    for _ in range(args.steps):
-        plan.run_device(proj.data_ptr(), vol.data_ptr(), stream.cuda_stream)
-    f1.record(stream)
-    torch.cuda.synchronize()
-    ms_plain = max_over_ranks(f0.elapsed_time(f1))
-    vol_host = vol.cpu().numpy() if rank == 0 else None
+    # same steps without per-launch events (overhead of the instrumentation);
+    # skipped when a step takes seconds
+    ms_plain = None
+    if ms_total / args.steps < 5000.0:
+        torch.cuda.synchronize()
+        f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        f0.record(stream)
+        for _ in range(args.steps):
+            plan.run_device(proj.data_ptr(), vol.data_ptr(), stream.cuda_stream)
+        f1.record(stream)
+        torch.cuda.synchronize()
+        ms_plain = max_over_ranks(f0.elapsed_time(f1))
+    # a volume above 8 GB is not copied back whole: the error check reads its
+    # middle slices, and the host path writes a ring of pinned frames
+    big = Nx * Nz * ny * 4 > (8 << 30)
+    y_mid = ny // 2
+    if rank != 0:
+        vol_host = None
+    elif big:
+        vol_host = None
+        vol_mid = vol[y_mid:y_mid + 2].cpu().numpy()
+    else:
+        vol_host = vol.cpu().numpy()
 
     # e2e through the host API: pinned frames in, pinned volume frames out
     pin_in = torch.from_numpy(frames).pin_memory()
-    pin_out = torch.empty((ny, Nz, Nx), dtype=torch.float32).pin_memory()
+    ring = 64 if big else ny
+    pin_out = torch.empty((ring, Nz, Nx), dtype=torch.float32).pin_memory()
     fin = [pin_in[t].numpy() for t in range(T)]
-    fout = [pin_out[y].numpy() for y in range(ny)]
+    fout = [pin_out[y % ring].numpy() for y in range(ny)]
     plan.run_host(fin, fout, stream.cuda_stream)  # warm the host-path buffers
     torch.cuda.synchronize()
     barrier()
@@ -318,7 +361,7 @@ def run_our_arm(args, c, rank, world, local_rank):
     torch.cuda.synchronize()
     barrier()
     ms_e2e = max_over_ranks(g0.elapsed_time(g1))
-    host_ok = bool(np.array_equal(pin_out.numpy(), vol_host)) if rank == 0 else True
+    host_ok = (bool(np.array_equal(pin_out.numpy(), vol_host)) if not big else None) if rank == 0 else True
 
     units = units_per_step(c)
     value = units * args.steps * world / (ms_total / 1e3) / 1e9
@@ -335,9 +378,10 @@ def run_our_arm(args, c, rank, world, local_rank):
     achieved = per_launch_bytes / (per_launch_ms / 1e3) / 1e9
     roof = {"bound": "hbm", "kernel": dname, "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
             "frac": achieved / peaks["hbm_gbs"], "peak_source": peaks["source"],
-            "traffic": profiled_traffic(dname, c["name"]),
+            "traffic": profiled_traffic(dname, c["name"], c["storage"]),
             "bytes_per_launch": per_launch_bytes, "ms_per_launch": per_launch_ms,
-            "units_per_s": d["units"] / (d["ms"] / 1e3)}
+            "units_per_s": d["units"] / (d["ms"] / 1e3),
+            "onchip": onchip_roof(dname, d, c["storage"], clk)}
     step_ms = ms_total / args.steps
     kernel_share = {k: {"launches": v["launches"], "ms": round(v["ms"], 3),
                         "share": round(v["ms"] / max(sum(x["ms"] for x in kstats.values()), 1e-9), 4),
@@ -350,22 +394,27 @@ def run_our_arm(args, c, rank, world, local_rank):
         "vs_baseline": None, "dtype": "f32" if c["storage"] == "f32" else f"{c['storage']}-storage/f32-accumulate",
         "data": "synthetic",
         "config": {"workload": c["label"], "name": c["name"], "storage": c["storage"], "nx": nx, "ny": ny, "tilts": T, "vol_z": Nz,
-                   "units_per_step": units, "slab_slices": plan.geom.slab_slices or "auto",
+                   "units_per_step": units, "slab_slices": plan.slab,
                    "l2": "inputs larger than L2 (projections 256 MB, volume 1.26 GB at the default workload)",
                    "parallelism": f"replicas x{world}"},
         "e2e": {"value": e2e_value, "unit": UNIT, "ms_per_step": ms_e2e / args.steps,
                 "h2d_bytes_per_step": int(frames.nbytes), "d2h_bytes_per_step": int(Nx * Nz * ny * 4),
-                "host_equals_device": host_ok},
+                "host_equals_device": host_ok,
+                "host_frames": "one pinned frame per slice" if not big else
+                               f"every slice copied out, into a ring of {ring} pinned frames"},
         "gpu_launches": int(launches_per_step * args.steps),
         "roofline": roof,
         "kernels": kernel_share,
-        "timing_overhead": (ms_total - ms_plain) / ms_plain,
+        "timing_overhead": (ms_total - ms_plain) / ms_plain if ms_plain else None,
         "clocks": clk,
     }
     if not args.no_cpu_baseline and world == 1:
         threads = os.cpu_count() or 1
         line["cpu_baseline"] = cpu_baseline(c, frames, threads)
-        line["error"] = error_vs_oracle(c, frames, vol_host)
+        if big:
+            line["error"] = error_vs_oracle(c, frames, None, mid=vol_mid)
+        else:
+            line["error"] = error_vs_oracle(c, frames, vol_host)
     print(json.dumps(line), flush=True)
     plan.close()
 
@@ -626,6 +675,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--storage", default="f32", choices=sorted(STORAGE),
                     help="staged-sinogram storage: f32, or f16 / bf16 with per-tilt scale (FP32 accumulation)")
+    ap.add_argument("--slab", type=int, default=0, help="slices per device batch (0: the plan's default)")
     ap.add_argument("--series", type=int, default=64, help="batch_uneven: number of series")
     ap.add_argument("--group", type=int, default=16, help="batch_uneven: series resident per graph launch")
     ap.add_argument("--branches", type=int, default=4, help="batch_uneven: parallel graph branches")
@@ -649,6 +699,7 @@ def main():
     local_rank = int(os.environ.get("LOCAL_RANK", 0))
     c = workload(args.workload, seed_offset=rank)
     c["storage"] = args.storage
+    c["slab"] = args.slab
     if args.storage != "f32":
         c["label"] += f"; {args.storage} storage with per-tilt scale, FP32 accumulation"
     if args.impl == "reference":
