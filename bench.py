@@ -69,6 +69,14 @@ def workload(name: str, seed_offset: int = 0) -> dict:
     elif name == "wbp_4k":
         c = synth.precision_4k(seed=3 + seed_offset)
         c.update(method="wbp", label="WBP 4096x4096x41 tilts, thickness 1200")
+    elif name == "sart_4k_rows":
+        # tuning case: the 4k geometry per slice, 256 rows
+        c = synth.precision_4k(seed=3 + seed_offset)
+        c.update(ny=256, method="sart", relax=0.0,
+                 label="SART 4096x256x41 tilts, thickness 1200, 15 iterations, 5 subsets")
+    elif name == "wbp_4k_rows":
+        c = synth.precision_4k(seed=3 + seed_offset)
+        c.update(ny=256, method="wbp", label="WBP 4096x256x41 tilts, thickness 1200")
     elif name == "sart_4k":
         c = synth.precision_4k(seed=3 + seed_offset)
         c.update(method="sart", relax=0.0, label="SART 4096x4096x41 tilts, thickness 1200, 15 iterations, 5 subsets")
