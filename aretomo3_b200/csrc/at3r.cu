@@ -55,6 +55,7 @@ bool factor_direct(int n, std::vector<int>& rad)
 }
 
 struct HostFft {
+    int rs = 0;          // radix set of its stages (radix_set_of)
     FftPlan plan{};
     float2* d_tables = nullptr;  // twiddles, chirp, bhat in one allocation
     size_t bytes = 0;
@@ -93,6 +94,18 @@ void host_fft_pow2(std::vector<std::complex<double>>& a, int sign)
 
 at3r_status dalloc_bytes(at3r_plan* p, void** ptr, size_t bytes);   // defined with the plan
 
+// Calls f with std::integral_constant<int, rs> for the kernels compiled for
+// radix set rs (see radix_set_of).
+template <class F>
+void dispatch_rs(int rs, F&& f)
+{
+    switch (rs) {
+        case 0: f(std::integral_constant<int, 0>{}); break;
+        case 1: f(std::integral_constant<int, 1>{}); break;
+        default: f(std::integral_constant<int, 2>{}); break;
+    }
+}
+
 // Per-stage divisors of the Stockham index arithmetic.
 void set_stage_divs(FftDirect& d)
 {
@@ -117,6 +130,8 @@ at3r_status make_fft(at3r_plan* pl, int n, HostFft& h)
         p.d.nst = (n == 1) ? 0 : (int)rad.size();
         for (int i = 0; i < p.d.nst; i++) p.d.radix[i] = rad[i];
         set_stage_divs(p.d);
+        h.rs = 0;
+        for (int i = 0; i < p.d.nst; i++) h.rs = std::max(h.rs, radix_set_of(p.d.radix[i]));
         fill_twiddles(tw, n);
     } else {
         int m = 1;
@@ -128,6 +143,7 @@ at3r_status make_fft(at3r_plan* pl, int n, HostFft& h)
         p.d.nst = (int)rad.size();
         for (int i = 0; i < p.d.nst; i++) p.d.radix[i] = rad[i];
         set_stage_divs(p.d);
+        h.rs = 0;   // a power of two
         fill_twiddles(tw, m);
         chirp.resize(n);
         std::vector<std::complex<double>> cd(n);
@@ -259,6 +275,7 @@ struct at3r_plan {
     HostFft fN, f2x, f2z, fz, fx;
     int zcrop_cb = 4, zcrop_pitch = 0;
     int b_rweight = 1, b_row = 1, b_xc2r = 1;   // sequences per CTA of the row FFT kernels
+    int rs_zcrop = 0;                           // radix set of the z-crop kernel (both its lengths)
     size_t smem_rweight = 0, smem_row = 0, smem_zcrop = 0, smem_xc2r = 0;
     int bp_ww_sart = 0, bp_ww_wbp = 0;
     // host path
@@ -458,9 +475,12 @@ at3r_status run_slab_t(at3r_plan* p, const float* proj, size_t tilt_stride, int 
     }
     // WBP
     TB(p, st);
-    k_rweight<ST><<<dim3(((T + 1) / 2 + p->b_rweight - 1) / p->b_rweight, S), 512, p->smem_rweight, st>>>(
-        proj, tilt_stride, p->nx, proj_y0, p->d_cs, T, N, Nz, p->d_h, p->fN.plan, p->b_rweight, filt, p->d_scale,
-        p->d_flags);
+    dispatch_rs(p->fN.rs, [&](auto R) {
+        k_rweight<ST, decltype(R)::value><<<dim3(((T + 1) / 2 + p->b_rweight - 1) / p->b_rweight, S), 512,
+                                            p->smem_rweight, st>>>(proj, tilt_stride, p->nx, proj_y0, p->d_cs, T, N,
+                                                                   Nz, p->d_h, p->fN.plan, p->b_rweight, filt,
+                                                                   p->d_scale, p->d_flags);
+    });
     TE(p, st, KK_RWEIGHT, (f4 + es) * S * T * N, (double)S * T * N);
     BpArgs a{};
     a.sino = filt; a.scale = p->d_scale; a.shadow = nullptr; a.T = T; a.N = N; a.t0 = 0; a.t1 = T; a.cs = p->d_cs;
@@ -471,19 +491,24 @@ at3r_status run_slab_t(at3r_plan* p, const float* proj, size_t tilt_stride, int 
     k_bp<1, ST, float, false><<<bgrid, BP_THREADS, bp_smem(T, a.ww), st>>>(a);
     TE(p, st, KK_BP_WBP, es * S * (double)T * N + f4 * 4 * vox, 4 * vox * T);
     TB(p, st);
-    k_row_r2c<<<dim3((Nz + p->b_row - 1) / p->b_row, S), 512, p->smem_row, st>>>(p->d_g2, Nx, Nz, p->f2x.plan,
-                                                                                   p->b_row, p->d_y);
+    dispatch_rs(p->f2x.rs, [&](auto R) {
+        k_row_r2c<decltype(R)::value><<<dim3((Nz + p->b_row - 1) / p->b_row, S), 512, p->smem_row, st>>>(
+            p->d_g2, Nx, Nz, p->f2x.plan, p->b_row, p->d_y);
+    });
     TE(p, st, KK_ROW_R2C, f4 * 4 * vox + 8.0 * S * 2 * Nz * KX, 4 * vox);
     const float norm = (float)(1.0 / (2.0 * Nx) / (2.0 * Nz));
     float2* w = reinterpret_cast<float2*>(p->d_g2);
     TB(p, st);
-    k_zcrop<<<dim3((KX + p->zcrop_cb - 1) / p->zcrop_cb, S), 512, p->smem_zcrop, st>>>(
-        p->d_y, Nx, Nz, p->zcrop_cb, p->zcrop_pitch, p->f2z.plan, p->fz.plan, norm, w);
+    dispatch_rs(p->rs_zcrop, [&](auto R) {
+        k_zcrop<decltype(R)::value><<<dim3((KX + p->zcrop_cb - 1) / p->zcrop_cb, S), 512, p->smem_zcrop, st>>>(
+            p->d_y, Nx, Nz, p->zcrop_cb, p->zcrop_pitch, p->f2z.plan, p->fz.plan, norm, w);
+    });
     TE(p, st, KK_ZCROP, 8.0 * S * 3 * Nz * KX, (double)S * 2 * Nz * KX);
     TB(p, st);
-    k_x_c2r<<<dim3(((Nz + 1) / 2 + p->b_xc2r - 1) / p->b_xc2r, S), 512, p->smem_xc2r, st>>>(
-        w, Nx, Nz, p->fx.plan, p->b_xc2r, p->c2r == AT3R_C2R_PACKED, vol,
-                                                              (size_t)Nx * Nz);
+    dispatch_rs(p->fx.rs, [&](auto R) {
+        k_x_c2r<decltype(R)::value><<<dim3(((Nz + 1) / 2 + p->b_xc2r - 1) / p->b_xc2r, S), 512, p->smem_xc2r, st>>>(
+            w, Nx, Nz, p->fx.plan, p->b_xc2r, p->c2r == AT3R_C2R_PACKED, vol, (size_t)Nx * Nz);
+    });
     TE(p, st, KK_XC2R, 8.0 * S * Nz * KX + f4 * vox, vox);
     return AT3R_OK;
 }
@@ -686,12 +711,19 @@ at3r_status plan_create_impl(const at3r_geom* g, cudaStream_t alloc_stream, at3r
         p->smem_zcrop = 2 * sizeof(float2) * p->zcrop_cb * p->zcrop_pitch;
         p->bp_ww_wbp = bp_window(BP_TX, BP_TZ, 0.5, cs, p->T);
         if (p->bp_ww_wbp > BP_WW) return fail(set_err(AT3R_ERR_TOO_LARGE, "back-projection window exceeds its stride"));
-        for (const void* fn : {(const void*)k_rweight<float>, (const void*)k_rweight<__half>,
-                               (const void*)k_rweight<__nv_bfloat16>})
-            if ((rc = set_smem(fn, p->smem_rweight))) return fail(rc);
-        if ((rc = set_smem((const void*)k_row_r2c, p->smem_row))) return fail(rc);
-        if ((rc = set_smem((const void*)k_zcrop, p->smem_zcrop))) return fail(rc);
-        if ((rc = set_smem((const void*)k_x_c2r, p->smem_xc2r))) return fail(rc);
+        p->rs_zcrop = std::max(p->f2z.rs, p->fz.rs);
+        std::vector<std::pair<const void*, size_t>> fns;
+        dispatch_rs(p->fN.rs, [&](auto R) {
+            constexpr int r = decltype(R)::value;
+            fns.push_back({(const void*)k_rweight<float, r>, p->smem_rweight});
+            fns.push_back({(const void*)k_rweight<__half, r>, p->smem_rweight});
+            fns.push_back({(const void*)k_rweight<__nv_bfloat16, r>, p->smem_rweight});
+        });
+        dispatch_rs(p->f2x.rs, [&](auto R) { fns.push_back({(const void*)k_row_r2c<decltype(R)::value>, p->smem_row}); });
+        dispatch_rs(p->rs_zcrop, [&](auto R) { fns.push_back({(const void*)k_zcrop<decltype(R)::value>, p->smem_zcrop}); });
+        dispatch_rs(p->fx.rs, [&](auto R) { fns.push_back({(const void*)k_x_c2r<decltype(R)::value>, p->smem_xc2r}); });
+        for (auto& f : fns)
+            if ((rc = set_smem(f.first, f.second))) return fail(rc);
         for (const void* fn : {(const void*)k_bp<1, float, float, false>, (const void*)k_bp<1, __half, float, false>,
                                (const void*)k_bp<1, __nv_bfloat16, float, false>})
             if ((rc = set_smem(fn, bp_smem(p->T, p->bp_ww_wbp)))) return fail(rc);

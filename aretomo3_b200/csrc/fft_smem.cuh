@@ -192,9 +192,14 @@ __device__ __forceinline__ void stockham_stage(const float2* __restrict__ in, fl
 #pragma unroll
         for (int r = 0; r < R; r++) v[r] = src[j + r * nb];
         if (Ns > 1) {
-            const int ts = twbase * jm;
+            // one table load; the higher twiddles as its powers
+            const float2 w1 = twiddle(d.tw, twbase * jm, sign);
+            float2 w = w1;
 #pragma unroll
-            for (int r = 1; r < R; r++) v[r] = cmul(v[r], twiddle(d.tw, r * ts, sign));
+            for (int r = 1; r < R; r++) {
+                v[r] = cmul(v[r], w);
+                if (r + 1 < R) w = cmul(w, w1);
+            }
         }
         Dft<R>::run(v, sign, d.tw, d.n);
         const int od = jq * Ns * R + jm;
@@ -203,8 +208,13 @@ __device__ __forceinline__ void stockham_stage(const float2* __restrict__ in, fl
     }
 }
 
+// Radix sets a kernel is compiled for (fewer radices, fewer registers):
+// 0 = {2, 4, 8}; 1 = {2, 3, 4, 5, 8}; 2 = every radix of the planner.
+__host__ __device__ constexpr int radix_set_of(int r) { return (r == 2 || r == 4 || r == 8) ? 0 : (r == 3 || r == 5) ? 1 : 2; }
+
 // Runs all stages, ping-ponging between a and b.  Returns the buffer that
 // holds the result.  All threads of the CTA must call it.
+template <int RS>
 __device__ inline float2* stockham(float2* a, float2* b, const FftDirect& d, int batch, int pitch, int sign)
 {
     int Ns = 1;
@@ -212,14 +222,19 @@ __device__ inline float2* stockham(float2* a, float2* b, const FftDirect& d, int
         const int R = d.radix[s];
         switch (R) {
             case 2: stockham_stage<2>(a, b, d, s, Ns, batch, pitch, sign); break;
-            case 3: stockham_stage<3>(a, b, d, s, Ns, batch, pitch, sign); break;
             case 4: stockham_stage<4>(a, b, d, s, Ns, batch, pitch, sign); break;
-            case 5: stockham_stage<5>(a, b, d, s, Ns, batch, pitch, sign); break;
-            case 7: stockham_stage<7>(a, b, d, s, Ns, batch, pitch, sign); break;
             case 8: stockham_stage<8>(a, b, d, s, Ns, batch, pitch, sign); break;
-            case 11: stockham_stage<11>(a, b, d, s, Ns, batch, pitch, sign); break;
-            case 13: stockham_stage<13>(a, b, d, s, Ns, batch, pitch, sign); break;
-            default: break;  // host planning never emits another radix
+            default:
+                if constexpr (RS >= 1) {
+                    if (R == 3) { stockham_stage<3>(a, b, d, s, Ns, batch, pitch, sign); break; }
+                    if (R == 5) { stockham_stage<5>(a, b, d, s, Ns, batch, pitch, sign); break; }
+                }
+                if constexpr (RS >= 2) {
+                    if (R == 7) { stockham_stage<7>(a, b, d, s, Ns, batch, pitch, sign); break; }
+                    if (R == 11) { stockham_stage<11>(a, b, d, s, Ns, batch, pitch, sign); break; }
+                    if (R == 13) { stockham_stage<13>(a, b, d, s, Ns, batch, pitch, sign); break; }
+                }
+                break;  // the host launches the radix set that holds every stage
         }
         __syncthreads();
         float2* t = a; a = b; b = t;
@@ -232,9 +247,10 @@ __device__ inline float2* stockham(float2* a, float2* b, const FftDirect& d, int
 // (pitch >= p.work).  b is scratch of the same shape.  The first p.n
 // elements of each sequence of the returned buffer hold the transform.
 // Caller must __syncthreads() between writing a and calling this.
+template <int RS>
 __device__ inline float2* fft_run(float2* a, float2* b, const FftPlan& p, int batch, int pitch, int sign)
 {
-    if (!p.bluestein) return stockham(a, b, p.d, batch, pitch, sign);
+    if (!p.bluestein) return stockham<RS>(a, b, p.d, batch, pitch, sign);
     const int n = p.n, m = p.d.n;
     // x_k -> x_k * c_k (forward) or conj(x_k) * c_k (inverse = conj of forward of conj), zero pad
     for (int idx = threadIdx.x; idx < m * batch; idx += blockDim.x) {
@@ -249,7 +265,7 @@ __device__ inline float2* fft_run(float2* a, float2* b, const FftPlan& p, int ba
         }
     }
     __syncthreads();
-    float2* r = stockham(a, b, p.d, batch, pitch, -1);
+    float2* r = stockham<RS>(a, b, p.d, batch, pitch, -1);
     float2* o = (r == a) ? b : a;
     for (int idx = threadIdx.x; idx < m * batch; idx += blockDim.x) {
         const int q = idx / m, k = idx - q * m;
@@ -257,7 +273,7 @@ __device__ inline float2* fft_run(float2* a, float2* b, const FftPlan& p, int ba
         s[k] = cmul(s[k], __ldg(p.bhat + k));
     }
     __syncthreads();
-    r = stockham(r, o, p.d, batch, pitch, +1);
+    r = stockham<RS>(r, o, p.d, batch, pitch, +1);
     for (int idx = threadIdx.x; idx < n * batch; idx += blockDim.x) {
         const int q = idx / n, k = idx - q * n;
         float2* s = r + (size_t)q * pitch;

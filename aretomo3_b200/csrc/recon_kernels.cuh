@@ -217,8 +217,8 @@ __global__ void __launch_bounds__(256) k_gather_weight(const float* __restrict__
 // B such pairs per CTA, transformed as one batch (B <= 8: one warp per row
 // for the 16-bit row scales).  Grid (ceil(ceil(T/2) / B), slices).
 // ---------------------------------------------------------------------------
-template <typename ST>
-__global__ void __launch_bounds__(512) k_rweight(const float* __restrict__ proj, size_t tilt_stride, int row_pitch,
+template <typename ST, int RS>
+__global__ void __launch_bounds__(512, RS < 2 ? 2 : 1) k_rweight(const float* __restrict__ proj, size_t tilt_stride, int row_pitch,
                                                  int y0, const float2* __restrict__ cs, int T, int N, int Nz,
                                                  const float* __restrict__ hhalf, const __grid_constant__ FftPlan plan, int B,
                                                  ST* __restrict__ out, float* __restrict__ scale,
@@ -244,7 +244,7 @@ __global__ void __launch_bounds__(512) k_rweight(const float* __restrict__ proj,
             aq[x] = make_float2(__ldg(s0 + x) * w0, two ? __ldg(s1 + x) * w1 : 0.f);
     }
     __syncthreads();
-    float2* r = fft_run(a, b, plan, nq, pitch, -1);
+    float2* r = fft_run<RS>(a, b, plan, nq, pitch, -1);
     for (int q = 0; q < nq; q++) {
         float2* rq = r + (size_t)q * pitch;
         for (int k = threadIdx.x; k < N; k += blockDim.x) {
@@ -254,7 +254,7 @@ __global__ void __launch_bounds__(512) k_rweight(const float* __restrict__ proj,
         }
     }
     __syncthreads();
-    float2* r2 = fft_run(r, r == a ? b : a, plan, nq, pitch, +1);
+    float2* r2 = fft_run<RS>(r, r == a ? b : a, plan, nq, pitch, +1);
     // row 2q + c of the CTA is tilt 2(pair0 + q) + c, component c of sequence q
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     if constexpr (!std::is_same<ST, float>::value) {
@@ -1008,7 +1008,8 @@ __global__ void __launch_bounds__(256) k_fill_empty(float* __restrict__ vol, siz
 // g: [slices][2Nz][2Nx]; y: [slices][2Nz][KX] with KX = Nx/2 + 1.
 // B row pairs per CTA.  Grid (ceil(Nz / B), slices).
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(512) k_row_r2c(const float* __restrict__ g, int Nx, int Nz, const __grid_constant__ FftPlan plan, int B,
+template <int RS>
+__global__ void __launch_bounds__(512, RS < 2 ? 2 : 1) k_row_r2c(const float* __restrict__ g, int Nx, int Nz, const __grid_constant__ FftPlan plan, int B,
                                                  float2* __restrict__ y)
 {
     extern __shared__ float2 fsm[];
@@ -1024,7 +1025,7 @@ __global__ void __launch_bounds__(512) k_row_r2c(const float* __restrict__ g, in
         for (int x = threadIdx.x; x < X2; x += blockDim.x) aq[x] = make_float2(__ldg(g0 + x), __ldg(g0 + X2 + x));
     }
     __syncthreads();
-    const float2* Zs = fft_run(a, b, plan, nq, pitch, -1);
+    const float2* Zs = fft_run<RS>(a, b, plan, nq, pitch, -1);
     for (int q = 0; q < nq; q++) {
         const float2* Z = Zs + (size_t)q * pitch;
         float2* y0 = y + ((size_t)ys * 2 * Nz + 2 * (pr0 + q)) * KX;
@@ -1045,7 +1046,8 @@ __global__ void __launch_bounds__(512) k_row_r2c(const float* __restrict__ g, in
 // MaUtil/CCufft2D.cpp:65-86), inverse FFT over Nz.  CB columns per CTA.
 // y: [slices][2Nz][KX] -> w: [slices][Nz][KX].  Grid (ceil(KX/CB), slices).
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(512) k_zcrop(const float2* __restrict__ y, int Nx, int Nz, int CB, int pitch,
+template <int RS>
+__global__ void __launch_bounds__(512, RS < 2 ? 2 : 1) k_zcrop(const float2* __restrict__ y, int Nx, int Nz, int CB, int pitch,
                                                const __grid_constant__ FftPlan p2, const __grid_constant__ FftPlan p1, float norm, float2* __restrict__ w)
 {
     extern __shared__ float2 fsm[];
@@ -1060,7 +1062,7 @@ __global__ void __launch_bounds__(512) k_zcrop(const float2* __restrict__ y, int
         a[(size_t)c * pitch + Z] = c < nc ? ysl[(size_t)Z * KX + kx0 + c] : make_float2(0.f, 0.f);
     }
     __syncthreads();
-    float2* F = fft_run(a, b, p2, CB, pitch, -1);
+    float2* F = fft_run<RS>(a, b, p2, CB, pitch, -1);
     float2* G = (F == a) ? b : a;
     for (int idx = threadIdx.x; idx < Nz * CB; idx += blockDim.x) {
         const int c = idx / Nz, kz = idx - c * Nz;
@@ -1069,7 +1071,7 @@ __global__ void __launch_bounds__(512) k_zcrop(const float2* __restrict__ y, int
         G[(size_t)c * pitch + kz] = make_float2(v.x * norm, v.y * norm);
     }
     __syncthreads();
-    float2* H = fft_run(G, F, p1, CB, pitch, +1);
+    float2* H = fft_run<RS>(G, F, p1, CB, pitch, +1);
     float2* wsl = w + (size_t)ys * Nz * KX;
     for (int idx = threadIdx.x; idx < Nz * CB; idx += blockDim.x) {
         const int z = idx / CB, c = idx - z * CB;
@@ -1088,7 +1090,8 @@ __global__ void __launch_bounds__(512) k_zcrop(const float2* __restrict__ y, int
 // w: [slices][Nz][KX] -> vol: [slices][Nz][Nx] (row Nz-1-z).  B row pairs per
 // CTA.  Grid (ceil(ceil(Nz/2) / B), slices).
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(512) k_x_c2r(const float2* __restrict__ w, int Nx, int Nz, const __grid_constant__ FftPlan plan, int B,
+template <int RS>
+__global__ void __launch_bounds__(512, RS < 2 ? 2 : 1) k_x_c2r(const float2* __restrict__ w, int Nx, int Nz, const __grid_constant__ FftPlan plan, int B,
                                                int packed, float* __restrict__ vol, size_t vol_slice)
 {
     extern __shared__ float2 fsm[];
@@ -1115,7 +1118,7 @@ __global__ void __launch_bounds__(512) k_x_c2r(const float2* __restrict__ w, int
         }
     }
     __syncthreads();
-    const float2* rs = fft_run(a, b, plan, nq, pitch, +1);
+    const float2* rs = fft_run<RS>(a, b, plan, nq, pitch, +1);
     for (int q = 0; q < nq; q++) {
         const int z0 = 2 * (pz0 + q);
         const bool two = z0 + 1 < Nz;
