@@ -281,6 +281,7 @@ struct at3r_plan {
     // host path
     float* d_proj_slab[2] = {nullptr, nullptr};
     float* d_vol_slab[2] = {nullptr, nullptr};
+    float* d_xyz_slab[2] = {nullptr, nullptr};   // XY-frame copy of a slab (output stage)
     cudaStream_t s_copy_in = nullptr, s_copy_out = nullptr;
     cudaEvent_t ev[8] = {};
     size_t ws_bytes = 0;
@@ -778,7 +779,7 @@ void at3r_plan_destroy(at3r_plan* p)
                       (void*)p->d_y})
         dfree(p, ptr);
     for (HostFft* f : {&p->fN, &p->f2x, &p->f2z, &p->fz, &p->fx}) dfree(p, f->d_tables);
-    for (int i = 0; i < 2; i++) { dfree(p, p->d_proj_slab[i]); dfree(p, p->d_vol_slab[i]); }
+    for (int i = 0; i < 2; i++) { dfree(p, p->d_proj_slab[i]); dfree(p, p->d_vol_slab[i]); dfree(p, p->d_xyz_slab[i]); }
     if (p->s_copy_in) cudaStreamDestroy(p->s_copy_in);
     if (p->s_copy_out) cudaStreamDestroy(p->s_copy_out);
     for (cudaEvent_t& e : p->ev) if (e) cudaEventDestroy(e);
@@ -800,13 +801,19 @@ at3r_status at3r_run_device(at3r_plan* p, const float* proj, float* vol, void* s
     return end_run(p, st);
 }
 
-at3r_status at3r_run_host(at3r_plan* p, const float* const* frames, float* const* vol_frames, void* stream)
+// The host path: slabs of projections in on one copy stream, reconstruction
+// on `stream`, volume out on another copy stream, two slabs in flight.  The
+// volume goes out as XZ frames (vol_frames) or, when vol_xyz is set, as the
+// XY frames of FlipVol(flip) in one contiguous buffer [Nz][ny][Nx].
+at3r_status run_host_impl(at3r_plan* p, const float* const* frames, float* const* vol_frames, float* vol_xyz,
+                          int flip, void* stream)
 {
-    if (!p || !frames || !vol_frames) return set_err(AT3R_ERR_INVALID_ARGUMENT, "null argument");
+    if (!p || !frames || (!vol_frames && !vol_xyz)) return set_err(AT3R_ERR_INVALID_ARGUMENT, "null argument");
     for (int t = 0; t < p->T; t++)
         if (!frames[t]) return set_err(AT3R_ERR_INVALID_ARGUMENT, "null tilt frame");
-    for (int y = 0; y < p->ny; y++)
-        if (!vol_frames[y]) return set_err(AT3R_ERR_INVALID_ARGUMENT, "null volume frame");
+    if (!vol_xyz)
+        for (int y = 0; y < p->ny; y++)
+            if (!vol_frames[y]) return set_err(AT3R_ERR_INVALID_ARGUMENT, "null volume frame");
     cudaStream_t st = (cudaStream_t)stream;
     const size_t S = p->slab, nx = p->nx, T = p->T, slice = (size_t)p->Nx * p->Nz;
     at3r_status rc;
@@ -819,6 +826,9 @@ at3r_status at3r_run_host(at3r_plan* p, const float* const* frames, float* const
         AT3R_CUDA(cudaStreamCreateWithFlags(&p->s_copy_out, cudaStreamNonBlocking));
         for (cudaEvent_t& e : p->ev) AT3R_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     }
+    if (vol_xyz && !p->d_xyz_slab[0])
+        for (int i = 0; i < 2; i++)
+            if ((rc = dalloc(p, &p->d_xyz_slab[i], S * slice))) return rc;
     if ((rc = begin_run(p, st))) return rc;
     // ev[0,1]: input slab i copied; ev[2,3]: slab i computed; ev[4,5]: output slab i copied out
     const int nslab = (p->ny + p->slab - 1) / p->slab;
@@ -838,16 +848,54 @@ at3r_status at3r_run_host(at3r_plan* p, const float* const* frames, float* const
         AT3R_CUDA(cudaStreamWaitEvent(st, p->ev[b], 0));
         if (k >= 2) AT3R_CUDA(cudaStreamWaitEvent(st, p->ev[4 + b], 0));
         if ((rc = run_slab(p, p->d_proj_slab[b], S * nx, 0, n, p->d_vol_slab[b], st))) return rc;
+        if (vol_xyz) {
+            k_flip_rows<<<dim3(p->Nz, n), 256, 0, st>>>(p->d_vol_slab[b], p->d_xyz_slab[b], p->Nz, p->Nx, flip,
+                                                        (size_t)n * p->Nx);
+            p->launches++;
+        }
         AT3R_CUDA(cudaEventRecord(p->ev[2 + b], st));
         AT3R_CUDA(cudaStreamWaitEvent(p->s_copy_out, p->ev[2 + b], 0));
-        for (int j = 0; j < n; j++)
-            AT3R_CUDA(cudaMemcpyAsync(vol_frames[y0 + j], p->d_vol_slab[b] + (size_t)j * slice, sizeof(float) * slice,
-                                      cudaMemcpyDeviceToHost, p->s_copy_out));
+        if (vol_xyz) {
+            // rows y0 .. y0+n of every XY frame: one strided copy
+            AT3R_CUDA(cudaMemcpy2DAsync(vol_xyz + (size_t)y0 * p->Nx, sizeof(float) * (size_t)p->ny * p->Nx,
+                                        p->d_xyz_slab[b], sizeof(float) * (size_t)n * p->Nx,
+                                        sizeof(float) * (size_t)n * p->Nx, p->Nz, cudaMemcpyDeviceToHost,
+                                        p->s_copy_out));
+        } else {
+            for (int j = 0; j < n; j++)
+                AT3R_CUDA(cudaMemcpyAsync(vol_frames[y0 + j], p->d_vol_slab[b] + (size_t)j * slice,
+                                          sizeof(float) * slice, cudaMemcpyDeviceToHost, p->s_copy_out));
+        }
         AT3R_CUDA(cudaEventRecord(p->ev[4 + b], p->s_copy_out));
     }
     AT3R_CUDA(cudaStreamWaitEvent(st, p->ev[4 + ((nslab - 1) & 1)], 0));
     if ((rc = end_run(p, st))) return rc;
     AT3R_CUDA(cudaStreamSynchronize(st));
+    return AT3R_OK;
+}
+
+at3r_status at3r_run_host(at3r_plan* p, const float* const* frames, float* const* vol_frames, void* stream)
+{
+    if (!vol_frames) return set_err(AT3R_ERR_INVALID_ARGUMENT, "null argument");
+    return run_host_impl(p, frames, vol_frames, nullptr, 0, stream);
+}
+
+at3r_status at3r_run_host_xyz(at3r_plan* p, const float* const* frames, float* vol_xyz, int flip, void* stream)
+{
+    if (!vol_xyz) return set_err(AT3R_ERR_INVALID_ARGUMENT, "null argument");
+    return run_host_impl(p, frames, nullptr, vol_xyz, flip != 0, stream);
+}
+
+at3r_status at3r_volume_xyz(const float* vol_xzy, int nx, int ny, int vol_z, int flip, float* vol_xyz, void* stream)
+{
+    if (!vol_xzy || !vol_xyz || nx < 2 || ny < 1 || vol_z < 1)
+        return set_err(AT3R_ERR_INVALID_ARGUMENT, "null buffer or empty volume");
+    const int Nx = nx & ~1;
+    if (Nx != nx) return set_err(AT3R_ERR_INVALID_ARGUMENT, "the volume width is even (nx & ~1 of the projections)");
+    if (vol_z > 65535 || ny > 65535) return set_err(AT3R_ERR_TOO_LARGE, "ny and vol_z must stay below 65536");
+    k_flip_rows<<<dim3(vol_z, ny), 256, 0, (cudaStream_t)stream>>>(vol_xzy, vol_xyz, vol_z, Nx, flip != 0,
+                                                                   (size_t)ny * Nx);
+    AT3R_CUDA(cudaGetLastError());
     return AT3R_OK;
 }
 

@@ -973,6 +973,23 @@ __global__ void __launch_bounds__(256) k_ungroup(const float4* __restrict__ w, f
 }
 
 // ---------------------------------------------------------------------------
+// Volume output stage, DataUtil/CTiltSeries.cpp:286-305 (FlipVol): the
+// reconstruction's XZ frames become XY frames.  in: S frames [Nz][Nx] (row zr
+// of frame s); out frame fz = (flip ? Nz-1-zr : zr) gets row s = in frame s
+// row zr, out[fz * frame_pitch + s * Nx + x].  Nx is even; rows move as
+// float2.  Grid (Nz, S).
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_flip_rows(const float* __restrict__ in, float* __restrict__ out, int Nz,
+                                                   int Nx, int flip, size_t frame_pitch)
+{
+    const int zr = blockIdx.x, s = blockIdx.y;
+    const int fz = flip ? Nz - 1 - zr : zr;
+    const float2* src = reinterpret_cast<const float2*>(in + ((size_t)s * Nz + zr) * Nx);
+    float2* dst = reinterpret_cast<float2*>(out + (size_t)fz * frame_pitch + (size_t)s * Nx);
+    for (int x = threadIdx.x; x < Nx / 2; x += blockDim.x) dst[x] = __ldg(src + x);
+}
+
+// ---------------------------------------------------------------------------
 // Replace any "-1e30" voxel of a flagged slice (MaUtil/GFillEmpty2D.cu runs
 // after SART, AreTomo/Recon/CTomoSart.cpp:88).  The reference copies a
 // time-seeded random valid voxel; this fills the slice's valid mean, which is

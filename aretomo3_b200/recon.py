@@ -54,6 +54,10 @@ _EXPORTS = {
     "at3r_run_device": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
     "at3r_run_host": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p),
                                      ctypes.POINTER(ctypes.c_void_p), ctypes.c_void_p]),
+    "at3r_run_host_xyz": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p), ctypes.c_void_p,
+                                         ctypes.c_int, ctypes.c_void_p]),
+    "at3r_volume_xyz": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                       ctypes.c_void_p, ctypes.c_void_p]),
     "at3r_get_rfactor": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double), ctypes.c_int]),
     "at3r_plan_workspace_bytes": (ctypes.c_size_t, [ctypes.c_void_p]),
     "at3r_plan_last_launches": (ctypes.c_int64, [ctypes.c_void_p]),
@@ -163,6 +167,19 @@ class Plan:
         fin = (ctypes.c_void_p * T)(*[f.ctypes.data for f in frames])
         fout = (ctypes.c_void_p * len(vol_frames))(*[v.ctypes.data for v in vol_frames])
         _check(lib().at3r_run_host(self._h, fin, fout, ctypes.c_void_p(stream)))
+
+    def run_host_xyz(self, frames, out: np.ndarray | None = None, flip: bool = True, stream: int = 0) -> np.ndarray:
+        """Reconstructs and returns the volume as XY frames [Nz][ny][Nx], as
+        CTiltSeries::FlipVol(flip) gives them (flip: frames in z order)."""
+        T = len(frames)
+        if out is None:
+            out = np.empty((self.vol_z, self.ny, self.Nx), np.float32)
+        if out.shape != (self.vol_z, self.ny, self.Nx) or out.dtype != np.float32 or not out.flags.c_contiguous:
+            raise ValueError("out must be a contiguous float32 array [vol_z][ny][Nx]")
+        fin = (ctypes.c_void_p * T)(*[f.ctypes.data for f in frames])
+        _check(lib().at3r_run_host_xyz(self._h, fin, ctypes.c_void_p(out.ctypes.data), int(bool(flip)),
+                                       ctypes.c_void_p(stream)))
+        return out
 
     def rfactor(self) -> np.ndarray:
         """Per iteration (sum|raw - fp|, sum|raw|) of the last run."""
@@ -365,6 +382,21 @@ class CDoSartRecon:
             return _host_run(plan, tilt_series.frames)
         finally:
             plan.close()
+
+
+def volume_xyz(vol, flip: bool = True, out=None, stream=None):
+    """Device transpose of a torch CUDA volume vol[ny][Nz][Nx] (XZ frames) to
+    XY frames [Nz][ny][Nx], as CTiltSeries::FlipVol(flip)."""
+    import torch
+    if not (vol.is_cuda and vol.dtype == torch.float32 and vol.is_contiguous() and vol.dim() == 3):
+        raise ValueError("vol must be a contiguous float32 CUDA tensor [ny][Nz][Nx]")
+    ny, nz, nx = vol.shape
+    if out is None:
+        out = torch.empty((nz, ny, nx), device=vol.device, dtype=torch.float32)
+    s = stream if stream is not None else torch.cuda.current_stream(vol.device)
+    _check(lib().at3r_volume_xyz(ctypes.c_void_p(vol.data_ptr()), nx, ny, nz, int(bool(flip)),
+                                 ctypes.c_void_p(out.data_ptr()), ctypes.c_void_p(s.cuda_stream)))
+    return out
 
 
 def reconstruct_device(proj, tilts, vol_z, method=WBP, out=None, stream=None, **kw):

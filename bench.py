@@ -371,6 +371,35 @@ def run_our_arm(args, c, rank, world, local_rank):
     ms_e2e = max_over_ranks(g0.elapsed_time(g1))
     host_ok = (bool(np.array_equal(pin_out.numpy(), vol_host)) if not big else None) if rank == 0 else True
 
+    # volume output stage (CTiltSeries::FlipVol): the XY-frame volume written by
+    # the host path directly, against XZ frames followed by the host-side flip
+    out_stage = None
+    if args.output == "xyz" and not big:
+        pin_xyz = torch.empty((Nz, ny, Nx), dtype=torch.float32).pin_memory()
+        xyz = pin_xyz.numpy()
+        plan.run_host_xyz(fin, out=xyz, flip=True)
+        torch.cuda.synchronize()
+        h0, h1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        h0.record(stream)
+        for _ in range(args.steps):
+            plan.run_host_xyz(fin, out=xyz, flip=True, stream=stream.cuda_stream)
+        h1.record(stream)
+        torch.cuda.synchronize()
+        ms_xyz = h0.elapsed_time(h1) / args.steps
+        # the reference's loop: one row copy per (z, y) into new frames
+        t = time.perf_counter()
+        flipped = np.empty((Nz, ny, Nx), np.float32)
+        src = pin_out.numpy()
+        for zr in range(Nz):
+            flipped[Nz - 1 - zr] = src[:, zr, :]
+        ms_flip = (time.perf_counter() - t) * 1e3
+        out_stage = {"xyz_e2e_ms_per_step": ms_xyz, "xzy_e2e_ms_per_step": ms_e2e / args.steps,
+                     "host_flipvol_ms": ms_flip, "equal": bool(np.array_equal(flipped, xyz)),
+                     "xyz_e2e_value": units_per_step(c) / (ms_xyz / 1e3) / 1e9,
+                     "note": "xyz: XY frames of FlipVol(1) written by the host path (device transpose per slab, "
+                             "one strided copy per slab); xzy + host_flipvol: XZ frames, then the reference's "
+                             "row-copy loop on one host thread"}
+
     units = units_per_step(c)
     value = units * args.steps * world / (ms_total / 1e3) / 1e9
     e2e_value = units * args.steps * world / (ms_e2e / 1e3) / 1e9
@@ -414,6 +443,7 @@ def run_our_arm(args, c, rank, world, local_rank):
         "roofline": roof,
         "kernels": kernel_share,
         "timing_overhead": (ms_total - ms_plain) / ms_plain if ms_plain else None,
+        "output_stage": out_stage,
         "clocks": clk,
     }
     if not args.no_cpu_baseline and world == 1:
@@ -684,6 +714,8 @@ def main():
     ap.add_argument("--storage", default="f32", choices=sorted(STORAGE),
                     help="staged-sinogram storage: f32, or f16 / bf16 with per-tilt scale (FP32 accumulation)")
     ap.add_argument("--slab", type=int, default=0, help="slices per device batch (0: the plan's default)")
+    ap.add_argument("--output", default="xzy", choices=["xzy", "xyz"],
+                    help="xyz: also time the volume output stage (XY frames, as FlipVol)")
     ap.add_argument("--series", type=int, default=64, help="batch_uneven: number of series")
     ap.add_argument("--group", type=int, default=16, help="batch_uneven: series resident per graph launch")
     ap.add_argument("--branches", type=int, default=4, help="batch_uneven: parallel graph branches")

@@ -136,6 +136,23 @@ at3r_status at3r_sart_device_noalloc(const float* proj, int nx, int ny, int n_ti
                                      int vol_z, int start_tilt, int num_tilts, int iterations, int subsets,
                                      float relax, float* vol, void* stream);
 
+/* Volume output stage (replaces CTiltSeries::FlipVol after the reconstruction,
+ * DataUtil/CTiltSeries.cpp:286-305, called from CAreTomoMain::mFlipVol,
+ * AreTomo/CAreTomoMain.cpp:893-903): the volume as XY frames.  Frame fz of
+ * the result is row zr of every XZ frame, fz = flip ? Nz-1-zr : zr, where row
+ * zr of an XZ frame holds z = Nz-1-zr; so flip = 1 (the reference's
+ * -FlipVol 1) gives frames in z order and flip = 0 (-FlipVol 2) in reverse
+ * z order.
+ *
+ * at3r_run_host_xyz: at3r_run_host, with the volume written as those XY
+ * frames into one contiguous host buffer vol_xyz[Nz][ny][Nx] (frame fz at
+ * vol_xyz + fz*ny*Nx); the transpose runs on the device per slab and each
+ * slab goes out as one strided copy.
+ * at3r_volume_xyz: the same transpose on device buffers, vol_xzy[ny][Nz][nx]
+ * -> vol_xyz[Nz][ny][nx] (nx = the volume width, even). */
+at3r_status at3r_run_host_xyz(at3r_plan* plan, const float* const* frames, float* vol_xyz, int flip, void* stream);
+at3r_status at3r_volume_xyz(const float* vol_xzy, int nx, int ny, int vol_z, int flip, float* vol_xyz, void* stream);
+
 /* Slab autotuner: times the reconstruction of the leading rows (at most two
  * full-capacity slabs) with slab sizes from 4 slices up to the plan's
  * workspace capacity (doubling) on proj / vol (device buffers in the layouts
