@@ -15,6 +15,7 @@
 #include <map>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 using namespace at3r;
@@ -282,6 +283,12 @@ struct at3r_plan {
     float* d_proj_slab[2] = {nullptr, nullptr};
     float* d_vol_slab[2] = {nullptr, nullptr};
     float* d_xyz_slab[2] = {nullptr, nullptr};   // XY-frame copy of a slab (output stage)
+    // pinned staging rings for pageable caller frames (input, output), borrowed
+    // from the process-wide staging pool for one run
+    char* h_stage_in[2] = {nullptr, nullptr};
+    char* h_stage_out[2] = {nullptr, nullptr};
+    cudaEvent_t ev_stage[4] = {};               // [0,1]: input ring slot free; [2,3]: output ring slot filled
+    bool pooled = false;                        // workspace from the library memory pool
     cudaStream_t s_copy_in = nullptr, s_copy_out = nullptr;
     cudaEvent_t ev[8] = {};
     size_t ws_bytes = 0;
@@ -300,12 +307,52 @@ namespace {
 // Workspace allocation: cudaMalloc, or — for plans made by the serving loop —
 // stream-ordered from the device's memory pool on the plan's allocation
 // stream, so that freeing it does not synchronise the device.
+// The library's device memory pool (one per device): plan workspaces come
+// from it and go back to it, so creating and destroying plans does not map
+// and unmap device memory each time (a cudaFree of a 1k SART plan's 7.5 GB
+// took 0.6 s).  at3r_release_cached_memory hands the pool's free memory back.
+struct DevicePool {
+    cudaMemPool_t pool = nullptr;
+    cudaStream_t stream = nullptr;
+};
+std::mutex g_pool_mu;
+std::map<int, DevicePool> g_pools;
+
+DevicePool* device_pool(int dev)
+{
+    std::lock_guard<std::mutex> lk(g_pool_mu);
+    DevicePool& dp = g_pools[dev];
+    if (!dp.pool) {
+        cudaMemPoolProps props{};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = dev;
+        if (cudaMemPoolCreate(&dp.pool, &props) != cudaSuccess) {
+            cudaGetLastError();
+            dp.pool = nullptr;
+            return nullptr;
+        }
+        uint64_t keep = UINT64_MAX;
+        cudaMemPoolSetAttribute(dp.pool, cudaMemPoolAttrReleaseThreshold, &keep);
+        if (cudaStreamCreateWithFlags(&dp.stream, cudaStreamNonBlocking) != cudaSuccess) {
+            cudaGetLastError();
+            cudaMemPoolDestroy(dp.pool);
+            dp.pool = nullptr;
+            return nullptr;
+        }
+    }
+    return &dp;
+}
+
 at3r_status dalloc_bytes(at3r_plan* p, void** ptr, size_t bytes)
 {
     cudaError_t e;
     if (p->alloc_stream) {
         e = cudaMallocAsync(ptr, bytes, p->alloc_stream);
         if (e == cudaSuccess) e = cudaStreamSynchronize(p->alloc_stream);
+    } else if (DevicePool* dp = p->pooled ? device_pool(p->device) : nullptr) {
+        e = cudaMallocFromPoolAsync(ptr, bytes, dp->pool, dp->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(dp->stream);
     } else {
         e = cudaMalloc(ptr, bytes);
     }
@@ -327,6 +374,7 @@ void dfree(at3r_plan* p, void* ptr)
 {
     if (!ptr) return;
     if (p->alloc_stream) cudaFreeAsync(ptr, p->alloc_stream);
+    else if (DevicePool* dp = p->pooled ? device_pool(p->device) : nullptr) cudaFreeAsync(ptr, dp->stream);
     else cudaFree(ptr);
 }
 
@@ -642,6 +690,7 @@ at3r_status plan_create_impl(const at3r_geom* g, cudaStream_t alloc_stream, at3r
     }
     at3r_plan* p = new at3r_plan();
     p->alloc_stream = alloc_stream;
+    p->pooled = alloc_stream == nullptr;
     p->g = *g;
     p->esz = g->storage == AT3R_STORE_F32 ? sizeof(float) : 2;
     p->tilts.assign(g->tilts_deg, g->tilts_deg + g->n_tilts);
@@ -773,6 +822,8 @@ at3r_status plan_create_impl(const at3r_geom* g, cudaStream_t alloc_stream, at3r
 void at3r_plan_destroy(at3r_plan* p)
 {
     if (!p) return;
+    // like cudaFree, wait for work that may still use the plan's memory
+    if (p->pooled) cudaDeviceSynchronize();
     for (void* ptr : {(void*)p->d_cs, (void*)p->d_raw, (void*)p->d_diff, (void*)p->d_scale, (void*)p->d_shadow,
                       (void*)p->d_w,
                       (void*)p->d_flags, (void*)p->d_rf, (void*)p->d_h, (void*)p->d_filt, (void*)p->d_g2,
@@ -783,6 +834,7 @@ void at3r_plan_destroy(at3r_plan* p)
     if (p->s_copy_in) cudaStreamDestroy(p->s_copy_in);
     if (p->s_copy_out) cudaStreamDestroy(p->s_copy_out);
     for (cudaEvent_t& e : p->ev) if (e) cudaEventDestroy(e);
+    for (cudaEvent_t& e : p->ev_stage) if (e) cudaEventDestroy(e);
     for (cudaEvent_t e : p->evpool) cudaEventDestroy(e);
     delete p;
 }
@@ -801,11 +853,219 @@ at3r_status at3r_run_device(at3r_plan* p, const float* proj, float* vol, void* s
     return end_run(p, st);
 }
 
+// Host <-> device staging for pageable caller memory.  A copy between the
+// device and pageable host memory runs at a fraction of the link's rate (the
+// driver stages it itself, synchronously); instead, data passes through two
+// pinned 64 MB ring slots, and the host side of each slot (pageable <->
+// pinned) is a parallel memcpy that overlaps the GPU's work.
+constexpr size_t kStageBytes = (size_t)64 << 20;
+
+bool host_pinned(const void* ptr)
+{
+    cudaPointerAttributes a{};
+    if (cudaPointerGetAttributes(&a, ptr) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeHost;
+}
+
+struct Piece {
+    char* dst;
+    const char* src;
+    size_t bytes;
+};
+
+// memcpy of every piece, split over up to 8 host threads (4 MB or more each)
+void parallel_copy(const std::vector<Piece>& pieces)
+{
+    size_t total = 0;
+    for (const Piece& pc : pieces) total += pc.bytes;
+    const unsigned hw = std::max(1u, std::min(8u, std::thread::hardware_concurrency()));
+    const size_t nt = std::min<size_t>(hw, std::max<size_t>(1, total >> 22));
+    auto run = [&](size_t lo, size_t hi) {
+        size_t off = 0;
+        for (const Piece& pc : pieces) {
+            const size_t a = std::max(lo, off), b = std::min(hi, off + pc.bytes);
+            if (a < b) std::memcpy(pc.dst + (a - off), pc.src + (a - off), b - a);
+            off += pc.bytes;
+            if (off >= hi) break;
+        }
+    };
+    if (nt <= 1) {
+        run(0, total);
+        return;
+    }
+    const size_t per = (total + nt - 1) / nt;
+    std::vector<std::thread> th;
+    for (size_t i = 1; i < nt; i++) th.emplace_back(run, i * per, std::min(total, (i + 1) * per));
+    run(0, std::min(total, per));
+    for (std::thread& t : th) t.join();
+}
+
+// Pieces of at most kStageBytes each, in order.
+std::vector<Piece> split_pieces(const std::vector<Piece>& in)
+{
+    std::vector<Piece> out;
+    for (const Piece& pc : in)
+        for (size_t o = 0; o < pc.bytes; o += kStageBytes)
+            out.push_back({pc.dst + o, pc.src + o, std::min(kStageBytes, pc.bytes - o)});
+    return out;
+}
+
+// Pinned staging sets (four 64 MB slots) shared by all plans of the process:
+// a run borrows one and returns it, so plans created per series do not pay
+// for pinned allocations (256 MB of cudaHostAlloc took longer than a 512^3
+// WBP).  The pool grows to the number of runs in flight at once.
+std::mutex g_stage_mu;
+std::vector<char*> g_stage_free;   // each entry: 4 * kStageBytes pinned
+
+char* stage_acquire()
+{
+    {
+        std::lock_guard<std::mutex> lk(g_stage_mu);
+        if (!g_stage_free.empty()) {
+            char* s = g_stage_free.back();
+            g_stage_free.pop_back();
+            return s;
+        }
+    }
+    char* s = nullptr;
+    if (cudaHostAlloc(reinterpret_cast<void**>(&s), 4 * kStageBytes, cudaHostAllocPortable) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    return s;
+}
+
+void stage_release(char* s)
+{
+    if (!s) return;
+    std::lock_guard<std::mutex> lk(g_stage_mu);
+    g_stage_free.push_back(s);
+}
+
+// Borrows a staging set for this run; the caller returns it with stage_return.
+at3r_status ensure_stage(at3r_plan* p)
+{
+    char* s = stage_acquire();
+    if (!s) return set_err(AT3R_ERR_OUT_OF_MEMORY, "pinned staging allocation failed");
+    for (int i = 0; i < 2; i++) {
+        p->h_stage_in[i] = s + i * kStageBytes;
+        p->h_stage_out[i] = s + (2 + i) * kStageBytes;
+    }
+    if (!p->ev_stage[0])
+        for (cudaEvent_t& e : p->ev_stage) AT3R_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    // the ring slots start free
+    for (int i = 0; i < 2; i++) AT3R_CUDA(cudaEventRecord(p->ev_stage[i], p->s_copy_in));
+    return AT3R_OK;
+}
+
+// Gives the borrowed set back once every copy through it has finished.
+void stage_return(at3r_plan* p)
+{
+    if (!p->h_stage_in[0]) return;
+    cudaStreamSynchronize(p->s_copy_in);
+    cudaStreamSynchronize(p->s_copy_out);
+    stage_release(p->h_stage_in[0]);
+    for (int i = 0; i < 2; i++) p->h_stage_in[i] = p->h_stage_out[i] = nullptr;
+}
+
+// Pageable host -> device: pieces (host src, device dst) through the input
+// ring on s_copy_in.  The host waits only for a ring slot's previous copy.
+at3r_status stage_in(at3r_plan* p, const std::vector<Piece>& pieces, int& slot)
+{
+    std::vector<Piece> chunk;
+    size_t used = 0;
+    auto flush = [&]() -> at3r_status {
+        if (chunk.empty()) return AT3R_OK;
+        AT3R_CUDA(cudaEventSynchronize(p->ev_stage[slot]));
+        char* st = p->h_stage_in[slot];
+        std::vector<Piece> host;
+        size_t o = 0;
+        for (const Piece& pc : chunk) {
+            host.push_back({st + o, pc.src, pc.bytes});
+            o += pc.bytes;
+        }
+        parallel_copy(host);
+        o = 0;
+        for (const Piece& pc : chunk) {
+            AT3R_CUDA(cudaMemcpyAsync(pc.dst, st + o, pc.bytes, cudaMemcpyHostToDevice, p->s_copy_in));
+            o += pc.bytes;
+        }
+        AT3R_CUDA(cudaEventRecord(p->ev_stage[slot], p->s_copy_in));
+        slot ^= 1;
+        chunk.clear();
+        used = 0;
+        return AT3R_OK;
+    };
+    at3r_status rc;
+    for (const Piece& pc : split_pieces(pieces)) {
+        if (used + pc.bytes > kStageBytes && (rc = flush())) return rc;
+        chunk.push_back(pc);
+        used += pc.bytes;
+    }
+    return flush();
+}
+
+// Device -> pageable host: pieces (device src, host dst) through the output
+// ring on s_copy_out; each filled slot is copied out on the host while the
+// next one fills.
+at3r_status stage_out(at3r_plan* p, const std::vector<Piece>& pieces)
+{
+    struct Pending {
+        int slot;
+        std::vector<Piece> host;
+    };
+    std::vector<Pending> pend;
+    auto drain = [&](Pending& d) -> at3r_status {
+        AT3R_CUDA(cudaEventSynchronize(p->ev_stage[2 + d.slot]));
+        parallel_copy(d.host);
+        return AT3R_OK;
+    };
+    std::vector<Piece> chunk;
+    size_t used = 0;
+    int slot = 0;
+    at3r_status rc;
+    auto flush = [&]() -> at3r_status {
+        if (chunk.empty()) return AT3R_OK;
+        if (pend.size() == 2) {   // the slot about to be filled must be copied out first
+            if ((rc = drain(pend.front()))) return rc;
+            pend.erase(pend.begin());
+        }
+        char* st = p->h_stage_out[slot];
+        Pending d{slot, {}};
+        size_t o = 0;
+        for (const Piece& pc : chunk) {
+            AT3R_CUDA(cudaMemcpyAsync(st + o, pc.src, pc.bytes, cudaMemcpyDeviceToHost, p->s_copy_out));
+            d.host.push_back({pc.dst, st + o, pc.bytes});
+            o += pc.bytes;
+        }
+        AT3R_CUDA(cudaEventRecord(p->ev_stage[2 + slot], p->s_copy_out));
+        pend.push_back(std::move(d));
+        slot ^= 1;
+        chunk.clear();
+        used = 0;
+        return AT3R_OK;
+    };
+    for (const Piece& pc : split_pieces(pieces)) {
+        if (used + pc.bytes > kStageBytes && (rc = flush())) return rc;
+        chunk.push_back(pc);
+        used += pc.bytes;
+    }
+    if ((rc = flush())) return rc;
+    for (Pending& d : pend)
+        if ((rc = drain(d))) return rc;
+    return AT3R_OK;
+}
+
 // The host path: slabs of projections in on one copy stream, reconstruction
 // on `stream`, volume out on another copy stream, two slabs in flight.  The
 // volume goes out as XZ frames (vol_frames) or, when vol_xyz is set, as the
-// XY frames of FlipVol(flip) in one contiguous buffer [Nz][ny][Nx].
-at3r_status run_host_impl(at3r_plan* p, const float* const* frames, float* const* vol_frames, float* vol_xyz,
+// XY frames of FlipVol(flip) in one contiguous buffer [Nz][ny][Nx].  Pinned
+// caller memory is copied directly; pageable memory through the staging
+// ring, the output of slab k drained on the host while slab k+1 computes.
+at3r_status run_host_body(at3r_plan* p, const float* const* frames, float* const* vol_frames, float* vol_xyz,
                           int flip, void* stream)
 {
     if (!p || !frames || (!vol_frames && !vol_xyz)) return set_err(AT3R_ERR_INVALID_ARGUMENT, "null argument");
@@ -829,16 +1089,54 @@ at3r_status run_host_impl(at3r_plan* p, const float* const* frames, float* const
     if (vol_xyz && !p->d_xyz_slab[0])
         for (int i = 0; i < 2; i++)
             if ((rc = dalloc(p, &p->d_xyz_slab[i], S * slice))) return rc;
+    const bool in_pinned = host_pinned(frames[0]);
+    const bool out_pinned = host_pinned(vol_xyz ? (const void*)vol_xyz : (const void*)vol_frames[0]);
+    if ((!in_pinned || !out_pinned) && (rc = ensure_stage(p))) return rc;
     if ((rc = begin_run(p, st))) return rc;
     // ev[0,1]: input slab i copied; ev[2,3]: slab i computed; ev[4,5]: output slab i copied out
     const int nslab = (p->ny + p->slab - 1) / p->slab;
+    int in_slot = 0;
     auto copy_in = [&](int k) -> at3r_status {
         const int b = k & 1, y0 = k * p->slab, n = std::min(p->slab, p->ny - y0);
         if (k >= 2) AT3R_CUDA(cudaStreamWaitEvent(p->s_copy_in, p->ev[2 + b], 0));
-        for (int t = 0; t < p->T; t++)
-            AT3R_CUDA(cudaMemcpyAsync(p->d_proj_slab[b] + (size_t)t * S * nx, frames[t] + (size_t)y0 * nx,
-                                      sizeof(float) * n * nx, cudaMemcpyHostToDevice, p->s_copy_in));
+        if (in_pinned) {
+            for (int t = 0; t < p->T; t++)
+                AT3R_CUDA(cudaMemcpyAsync(p->d_proj_slab[b] + (size_t)t * S * nx, frames[t] + (size_t)y0 * nx,
+                                          sizeof(float) * n * nx, cudaMemcpyHostToDevice, p->s_copy_in));
+        } else {
+            std::vector<Piece> pc;
+            for (int t = 0; t < p->T; t++)
+                pc.push_back({reinterpret_cast<char*>(p->d_proj_slab[b] + (size_t)t * S * nx),
+                              reinterpret_cast<const char*>(frames[t] + (size_t)y0 * nx), sizeof(float) * n * nx});
+            at3r_status r2 = stage_in(p, pc, in_slot);
+            if (r2) return r2;
+        }
         AT3R_CUDA(cudaEventRecord(p->ev[b], p->s_copy_in));
+        return AT3R_OK;
+    };
+    // output of slab k: pieces (device src, host dst)
+    auto out_pieces = [&](int k) {
+        const int b = k & 1, y0 = k * p->slab, n = std::min(p->slab, p->ny - y0);
+        std::vector<Piece> pc;
+        if (vol_xyz) {
+            for (int fz = 0; fz < p->Nz; fz++)
+                pc.push_back({reinterpret_cast<char*>(vol_xyz + ((size_t)fz * p->ny + y0) * p->Nx),
+                              reinterpret_cast<const char*>(p->d_xyz_slab[b] + (size_t)fz * n * p->Nx),
+                              sizeof(float) * (size_t)n * p->Nx});
+        } else {
+            for (int j = 0; j < n; j++)
+                pc.push_back({reinterpret_cast<char*>(vol_frames[y0 + j]),
+                              reinterpret_cast<const char*>(p->d_vol_slab[b] + (size_t)j * slice),
+                              sizeof(float) * slice});
+        }
+        return pc;
+    };
+    auto drain_out = [&](int k) -> at3r_status {
+        const int b = k & 1;
+        AT3R_CUDA(cudaStreamWaitEvent(p->s_copy_out, p->ev[2 + b], 0));
+        at3r_status r2 = stage_out(p, out_pieces(k));
+        if (r2) return r2;
+        AT3R_CUDA(cudaEventRecord(p->ev[4 + b], p->s_copy_out));
         return AT3R_OK;
     };
     if ((rc = copy_in(0))) return rc;
@@ -854,6 +1152,11 @@ at3r_status run_host_impl(at3r_plan* p, const float* const* frames, float* const
             p->launches++;
         }
         AT3R_CUDA(cudaEventRecord(p->ev[2 + b], st));
+        if (!out_pinned) {
+            // slab k computes while the host drains slab k - 1
+            if (k >= 1 && (rc = drain_out(k - 1))) return rc;
+            continue;
+        }
         AT3R_CUDA(cudaStreamWaitEvent(p->s_copy_out, p->ev[2 + b], 0));
         if (vol_xyz) {
             // rows y0 .. y0+n of every XY frame: one strided copy
@@ -868,10 +1171,39 @@ at3r_status run_host_impl(at3r_plan* p, const float* const* frames, float* const
         }
         AT3R_CUDA(cudaEventRecord(p->ev[4 + b], p->s_copy_out));
     }
+    if (!out_pinned && (rc = drain_out(nslab - 1))) return rc;
     AT3R_CUDA(cudaStreamWaitEvent(st, p->ev[4 + ((nslab - 1) & 1)], 0));
     if ((rc = end_run(p, st))) return rc;
     AT3R_CUDA(cudaStreamSynchronize(st));
     return AT3R_OK;
+}
+
+at3r_status run_host_impl(at3r_plan* p, const float* const* frames, float* const* vol_frames, float* vol_xyz,
+                          int flip, void* stream)
+{
+    const at3r_status rc = run_host_body(p, frames, vol_frames, vol_xyz, flip, stream);
+    if (p) stage_return(p);
+    return rc;
+}
+
+void at3r_release_cached_memory(void)
+{
+    std::lock_guard<std::mutex> lk(g_pool_mu);
+    for (auto& kv : g_pools)
+        if (kv.second.pool) {
+            int dev = 0;
+            cudaGetDevice(&dev);
+            cudaSetDevice(kv.first);
+            cudaStreamSynchronize(kv.second.stream);
+            cudaMemPoolTrimTo(kv.second.pool, 0);
+            cudaSetDevice(dev);
+        }
+    {
+        std::lock_guard<std::mutex> lk2(g_stage_mu);
+        for (char* st : g_stage_free) cudaFreeHost(st);
+        g_stage_free.clear();
+    }
+    cudaGetLastError();
 }
 
 at3r_status at3r_run_host(at3r_plan* p, const float* const* frames, float* const* vol_frames, void* stream)

@@ -82,6 +82,7 @@ _EXPORTS = {
                                         ctypes.POINTER(ctypes.c_double)]),
     "at3r_server_in_use_bytes": (ctypes.c_size_t, [ctypes.c_void_p]),
     "at3r_server_destroy": (None, [ctypes.c_void_p]),
+    "at3r_release_cached_memory": (None, []),
     "at3r_status_str": (ctypes.c_char_p, [ctypes.c_int]),
     "at3r_last_error": (ctypes.c_char_p, []),
 }

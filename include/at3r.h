@@ -93,7 +93,11 @@ at3r_status at3r_run_device(at3r_plan* plan, const float* proj, float* vol, void
 
 /* Host form (the reference's CDoWbpRecon/CDoSartRecon data flow): reads the
  * tilt frames from host memory, writes the volume frames to host memory,
- * overlapping copies with compute; returns after the volume is on the host. */
+ * overlapping copies with compute; returns after the volume is on the host.
+ * Pinned frames are copied directly; pageable ones (plain new[] / malloc, as
+ * CTiltSeries allocates them) pass through a pinned staging ring with
+ * multi-threaded host copies that overlap the GPU.  destroying a plan waits
+ * for the device, as cudaFree does. */
 at3r_status at3r_run_host(at3r_plan* plan, const float* const* frames, float* const* vol_frames, void* stream);
 
 /* SART residual sums of the last run: per iteration, sum|raw - fp| and
@@ -135,6 +139,12 @@ int at3r_plan_c2r(const at3r_plan* plan);
 at3r_status at3r_sart_device_noalloc(const float* proj, int nx, int ny, int n_tilts, const float* tilts_deg,
                                      int vol_z, int start_tilt, int num_tilts, int iterations, int subsets,
                                      float relax, float* vol, void* stream);
+
+/* Plans take their device workspace from a memory pool of the library (one
+ * per device) that keeps freed blocks for the next plan, so creating and
+ * destroying plans per series costs no device mapping.  This returns the
+ * pool's free blocks to the device. */
+void at3r_release_cached_memory(void);
 
 /* Volume output stage (replaces CTiltSeries::FlipVol after the reconstruction,
  * DataUtil/CTiltSeries.cpp:286-305, called from CAreTomoMain::mFlipVol,
