@@ -279,7 +279,6 @@ def run_reference_arm(args, c, rank, world):
 def run_our_arm(args, c, rank, world, local_rank):
     import torch
     from aretomo3_b200 import recon, synth
-    dist = world > 1
     dev = torch.device("cuda", local_rank)
     torch.cuda.set_device(dev)
     frames = synth.make_tilt_series(c["nx"], c["ny"], c["tilts"], c["vol_z"], c["phantom"])
@@ -291,16 +290,11 @@ def run_our_arm(args, c, rank, world, local_rank):
     proj = torch.from_numpy(frames).to(dev)
     vol = torch.empty((ny, Nz, Nx), device=dev, dtype=torch.float32)
 
-    def barrier():
-        if dist:
-            torch.distributed.barrier()
+    from aretomo3_b200 import ranks
+    barrier = ranks.barrier
 
     def max_over_ranks(x: float) -> float:
-        if not dist:
-            return x
-        t = torch.tensor([x], device=dev, dtype=torch.float64)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        return float(t.item())
+        return ranks.max_over_ranks(x, device=dev)
 
     for _ in range(args.warmup):
         plan.run_device(proj.data_ptr(), vol.data_ptr(), stream.cuda_stream)
@@ -401,8 +395,8 @@ def run_our_arm(args, c, rank, world, local_rank):
                              "row-copy loop on one host thread"}
 
     units = units_per_step(c)
-    value = units * args.steps * world / (ms_total / 1e3) / 1e9
-    e2e_value = units * args.steps * world / (ms_e2e / 1e3) / 1e9
+    value = ranks.aggregate_rate(units, args.steps, world, ms_total) / 1e9
+    e2e_value = ranks.aggregate_rate(units, args.steps, world, ms_e2e) / 1e9
 
     if rank != 0:
         return
@@ -734,9 +728,8 @@ def main():
                 args.storage = "f16"
             run_serving_arm(args)
         return
-    rank = int(os.environ.get("RANK", 0))
-    world = int(os.environ.get("WORLD_SIZE", 1))
-    local_rank = int(os.environ.get("LOCAL_RANK", 0))
+    from aretomo3_b200 import ranks
+    rank, world, local_rank = ranks.rank_env()
     c = workload(args.workload, seed_offset=rank)
     c["storage"] = args.storage
     c["slab"] = args.slab
