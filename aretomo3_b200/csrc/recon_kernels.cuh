@@ -819,6 +819,30 @@ __global__ void __launch_bounds__(256) k_fp_diff(const float* __restrict__ vol, 
             const int o = (int)((unsigned)__float_as_int(tX) - (unsigned)__float_as_int(tZ) * (unsigned)Nx + kx);
             const float ux = 1.f - wx, uz = 1.f - wz;
             const float w00 = ux * uz, w10 = wx * uz, w01 = ux * wz, w11 = wx * wz;
+            if constexpr (std::is_same<VT, __half>::value) {
+                // FP16 shadow: the sample value of two slices per half2
+                // instruction, converted once and summed in FP32
+                const uint2 b00 = __ldg(reinterpret_cast<const uint2*>(g0 + o));
+                const uint2 b10 = __ldg(reinterpret_cast<const uint2*>(g0 + o + 1));
+                const uint2 b01 = __ldg(reinterpret_cast<const uint2*>(g1 + o));
+                const uint2 b11 = __ldg(reinterpret_cast<const uint2*>(g1 + o + 1));
+                const __half2 h00 = __float2half2_rn(w00), h10 = __float2half2_rn(w10);
+                const __half2 h01 = __float2half2_rn(w01), h11 = __float2half2_rn(w11);
+                __half2 lo = __hmul2(h00, from_bits<__half2>(b00.x));
+                __half2 hi = __hmul2(h00, from_bits<__half2>(b00.y));
+                lo = __hfma2(h10, from_bits<__half2>(b10.x), lo);
+                hi = __hfma2(h10, from_bits<__half2>(b10.y), hi);
+                lo = __hfma2(h01, from_bits<__half2>(b01.x), lo);
+                hi = __hfma2(h01, from_bits<__half2>(b01.y), hi);
+                lo = __hfma2(h11, from_bits<__half2>(b11.x), lo);
+                hi = __hfma2(h11, from_bits<__half2>(b11.y), hi);
+                const float2 flo = __half22float2(lo), fhi = __half22float2(hi);
+                fSum[0] += flo.x;
+                fSum[1] += flo.y;
+                fSum[2] += fhi.x;
+                fSum[3] += fhi.y;
+                continue;
+            }
             const float4 a00 = Quad<VT>::ld(g0 + o), a10 = Quad<VT>::ld(g0 + o + 1);
             const float4 a01 = Quad<VT>::ld(g1 + o), a11 = Quad<VT>::ld(g1 + o + 1);
             fSum[0] = __fmaf_rn(w11, a11.x, __fmaf_rn(w01, a01.x, __fmaf_rn(w10, a10.x, __fmaf_rn(w00, a00.x, fSum[0]))));
