@@ -144,6 +144,27 @@ __device__ __forceinline__ float comp(const float4& v, int q)
     return q == 0 ? v.x : q == 1 ? v.y : q == 2 ? v.z : v.w;
 }
 
+// for (i = threadIdx.x; i < n; i += blockDim.x) st(i, ld(i)), U iterations at
+// a time with their loads issued before their stores, so a thread waits for
+// global memory once per U elements rather than once per element.
+template <int U, class Ld, class St>
+__device__ __forceinline__ void staged_copy(int n, Ld ld, St st)
+{
+    for (int i0 = threadIdx.x; i0 < n; i0 += U * blockDim.x) {
+        decltype(ld(0)) v[U];
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            const int i = i0 + u * blockDim.x;
+            if (i < n) v[u] = ld(i);
+        }
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            const int i = i0 + u * blockDim.x;
+            if (i < n) st(i, v[u]);
+        }
+    }
+}
+
 // Largest magnitude over a CTA's values (non-empty ones only); every thread
 // gets the result.  Uses red[32] of shared memory.
 __device__ __forceinline__ float block_absmax(float v, float* red)
@@ -240,8 +261,8 @@ __global__ void __launch_bounds__(512, RS < 2 ? 2 : 1) k_rweight(const float* __
         const float* s0 = srow + (size_t)t0 * tilt_stride;
         const float* s1 = srow + (size_t)(two ? t1 : t0) * tilt_stride;
         float2* aq = a + (size_t)q * pitch;
-        for (int x = threadIdx.x; x < N; x += blockDim.x)
-            aq[x] = make_float2(__ldg(s0 + x) * w0, two ? __ldg(s1 + x) * w1 : 0.f);
+        staged_copy<4>(N, [&](int x) { return make_float2(__ldg(s0 + x) * w0, two ? __ldg(s1 + x) * w1 : 0.f); },
+                       [&](int x, float2 v) { aq[x] = v; });
     }
     __syncthreads();
     float2* r = fft_run<RS>(a, b, plan, nq, pitch, -1);
@@ -1063,7 +1084,8 @@ __global__ void __launch_bounds__(512, RS < 2 ? 2 : 1) k_row_r2c(const float* __
     for (int q = 0; q < nq; q++) {
         const float* g0 = g + ((size_t)ys * 2 * Nz + 2 * (pr0 + q)) * X2;
         float2* aq = a + (size_t)q * pitch;
-        for (int x = threadIdx.x; x < X2; x += blockDim.x) aq[x] = make_float2(__ldg(g0 + x), __ldg(g0 + X2 + x));
+        staged_copy<4>(X2, [&](int x) { return make_float2(__ldg(g0 + x), __ldg(g0 + X2 + x)); },
+                       [&](int x, float2 v) { aq[x] = v; });
     }
     __syncthreads();
     const float2* Zs = fft_run<RS>(a, b, plan, nq, pitch, -1);
@@ -1098,10 +1120,15 @@ __global__ void __launch_bounds__(512, RS < 2 ? 2 : 1) k_zcrop(const float2* __r
     float2* a = fsm;
     float2* b = fsm + (size_t)CB * pitch;
     const float2* ysl = y + (size_t)ys * Z2 * KX;
-    for (int idx = threadIdx.x; idx < Z2 * CB; idx += blockDim.x) {
-        const int Z = idx / CB, c = idx - Z * CB;
-        a[(size_t)c * pitch + Z] = c < nc ? ysl[(size_t)Z * KX + kx0 + c] : make_float2(0.f, 0.f);
-    }
+    staged_copy<4>(Z2 * CB,
+                   [&](int idx) {
+                       const int Z = idx / CB, c = idx - Z * CB;
+                       return c < nc ? __ldg(ysl + (size_t)Z * KX + kx0 + c) : make_float2(0.f, 0.f);
+                   },
+                   [&](int idx, float2 v) {
+                       const int Z = idx / CB, c = idx - Z * CB;
+                       a[(size_t)c * pitch + Z] = v;
+                   });
     __syncthreads();
     float2* F = fft_run<RS>(a, b, p2, CB, pitch, -1);
     float2* G = (F == a) ? b : a;
@@ -1148,15 +1175,17 @@ __global__ void __launch_bounds__(512, RS < 2 ? 2 : 1) k_x_c2r(const float2* __r
         const float2* A = w + ((size_t)ys * Nz + z0) * KX;
         const float2* Bv = A + KX;
         float2* aq = a + (size_t)q * pitch;
-        for (int k = threadIdx.x; k < Nx; k += blockDim.x) {
-            const bool lo = k <= H;
-            const int kk = lo ? k : Nx - k;
-            float2 av = A[kk];
-            float2 bv = two ? Bv[kk] : make_float2(0.f, 0.f);
-            if (kk == 0 || kk == H) { av.y = 0.f; bv.y = 0.f; }
-            if (!lo) { av.y = -av.y; bv.y = -bv.y; }
-            aq[k] = make_float2(av.x - bv.y, av.y + bv.x);   // A + iB
-        }
+        staged_copy<4>(Nx,
+                       [&](int k) {
+                           const bool lo = k <= H;
+                           const int kk = lo ? k : Nx - k;
+                           float2 av = __ldg(A + kk);
+                           float2 bv = two ? __ldg(Bv + kk) : make_float2(0.f, 0.f);
+                           if (kk == 0 || kk == H) { av.y = 0.f; bv.y = 0.f; }
+                           if (!lo) { av.y = -av.y; bv.y = -bv.y; }
+                           return make_float2(av.x - bv.y, av.y + bv.x);   // A + iB
+                       },
+                       [&](int k, float2 v) { aq[k] = v; });
     }
     __syncthreads();
     const float2* rs = fft_run<RS>(a, b, plan, nq, pitch, +1);
