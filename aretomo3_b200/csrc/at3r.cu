@@ -746,16 +746,16 @@ at3r_status plan_create_impl(const at3r_geom* g, cudaStream_t alloc_stream, at3r
         auto batch = [](int work) {
             int b = 1;
             while (b < 8 && (size_t)work * b * 2 <= 4096) b *= 2;
-            while (b > 1 && 2 * sizeof(float2) * (size_t)work * b > (96u << 10)) b /= 2;
+            while (b > 1 && 2 * sizeof(float2) * (size_t)fft_pitch(work) * b > (96u << 10)) b /= 2;
             return b;
         };
         p->b_rweight = batch(p->fN.plan.work);
         p->b_row = batch(p->f2x.plan.work);
         p->b_xc2r = batch(p->fx.plan.work);
-        p->smem_rweight = 2 * sizeof(float2) * p->fN.plan.work * p->b_rweight;
-        p->smem_row = 2 * sizeof(float2) * p->f2x.plan.work * p->b_row;
-        p->smem_xc2r = 2 * sizeof(float2) * p->fx.plan.work * p->b_xc2r;
-        p->zcrop_pitch = round_up(std::max(p->f2z.plan.work, p->fz.plan.work), 2) + 1;
+        p->smem_rweight = 2 * sizeof(float2) * fft_pitch(p->fN.plan.work) * p->b_rweight;
+        p->smem_row = 2 * sizeof(float2) * fft_pitch(p->f2x.plan.work) * p->b_row;
+        p->smem_xc2r = 2 * sizeof(float2) * fft_pitch(p->fx.plan.work) * p->b_xc2r;
+        p->zcrop_pitch = round_up(fft_pitch(std::max(p->f2z.plan.work, p->fz.plan.work)), 2) + 1;
         p->zcrop_cb = std::max(4, std::min(32, 4096 / (2 * p->Nz)));
         while (p->zcrop_cb > 1 && 2 * sizeof(float2) * p->zcrop_cb * p->zcrop_pitch > 227 * 1024) p->zcrop_cb /= 2;
         p->smem_zcrop = 2 * sizeof(float2) * p->zcrop_cb * p->zcrop_pitch;

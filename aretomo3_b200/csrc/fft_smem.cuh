@@ -20,6 +20,13 @@ namespace at3r {
 
 constexpr int kMaxFftStages = 32;
 
+// Sequences sit in shared memory with one spare element after every 16, so
+// that the stride-R writes of the early Stockham stages (and other strided
+// patterns) spread over the banks: element i of a sequence is at fft_pad(i).
+__host__ __device__ constexpr int fft_pad(int i) { return i + (i >> 4); }
+// Elements one padded sequence of length n occupies.
+__host__ __device__ constexpr int fft_pitch(int n) { return n + ((n - 1) >> 4) + 1; }
+
 struct FftDirect {
     int n;                       // length
     int nst;                     // number of stages
@@ -172,7 +179,7 @@ template <> struct Dft<11> : DftGeneric<11> {};
 template <> struct Dft<13> : DftGeneric<13> {};
 
 // One Stockham stage of radix R over `batch` sequences of length d.n stored
-// with pitch `pitch` (complex elements).
+// with pitch `pitch` (complex elements), element i at fft_pad(i).
 template <int R>
 __device__ __forceinline__ void stockham_stage(const float2* __restrict__ in, float2* __restrict__ out,
                                                const FftDirect& d, int st, int Ns, int batch, int pitch, int sign)
@@ -190,7 +197,7 @@ __device__ __forceinline__ void stockham_stage(const float2* __restrict__ in, fl
         const int jm = j - jq * Ns;
         float2 v[R];
 #pragma unroll
-        for (int r = 0; r < R; r++) v[r] = src[j + r * nb];
+        for (int r = 0; r < R; r++) v[r] = src[fft_pad(j + r * nb)];
         if (Ns > 1) {
             // one table load; the higher twiddles as its powers
             const float2 w1 = twiddle(d.tw, twbase * jm, sign);
@@ -204,7 +211,7 @@ __device__ __forceinline__ void stockham_stage(const float2* __restrict__ in, fl
         Dft<R>::run(v, sign, d.tw, d.n);
         const int od = jq * Ns * R + jm;
 #pragma unroll
-        for (int r = 0; r < R; r++) dst[od + r * Ns] = v[r];
+        for (int r = 0; r < R; r++) dst[fft_pad(od + r * Ns)] = v[r];
     }
 }
 
@@ -244,7 +251,7 @@ __device__ inline float2* stockham(float2* a, float2* b, const FftDirect& d, int
 }
 
 // FFT of `batch` sequences of length p.n, each starting at a + q*pitch
-// (pitch >= p.work).  b is scratch of the same shape.  The first p.n
+// (pitch >= fft_pitch(p.work)), element i at fft_pad(i).  b is scratch of the same shape.  The first p.n
 // elements of each sequence of the returned buffer hold the transform.
 // Caller must __syncthreads() between writing a and calling this.
 template <int RS>
@@ -257,11 +264,11 @@ __device__ inline float2* fft_run(float2* a, float2* b, const FftPlan& p, int ba
         const int q = idx / m, k = idx - q * m;
         float2* s = a + (size_t)q * pitch;
         if (k < n) {
-            float2 x = s[k];
+            float2 x = s[fft_pad(k)];
             if (sign > 0) x = cconj(x);
-            s[k] = cmul(x, __ldg(p.chirp + k));
+            s[fft_pad(k)] = cmul(x, __ldg(p.chirp + k));
         } else {
-            s[k] = make_float2(0.f, 0.f);
+            s[fft_pad(k)] = make_float2(0.f, 0.f);
         }
     }
     __syncthreads();
@@ -270,15 +277,15 @@ __device__ inline float2* fft_run(float2* a, float2* b, const FftPlan& p, int ba
     for (int idx = threadIdx.x; idx < m * batch; idx += blockDim.x) {
         const int q = idx / m, k = idx - q * m;
         float2* s = r + (size_t)q * pitch;
-        s[k] = cmul(s[k], __ldg(p.bhat + k));
+        s[fft_pad(k)] = cmul(s[fft_pad(k)], __ldg(p.bhat + k));
     }
     __syncthreads();
     r = stockham<RS>(r, o, p.d, batch, pitch, +1);
     for (int idx = threadIdx.x; idx < n * batch; idx += blockDim.x) {
         const int q = idx / n, k = idx - q * n;
         float2* s = r + (size_t)q * pitch;
-        float2 y = cmul(s[k], __ldg(p.chirp + k));
-        s[k] = sign > 0 ? cconj(y) : y;
+        float2 y = cmul(s[fft_pad(k)], __ldg(p.chirp + k));
+        s[fft_pad(k)] = sign > 0 ? cconj(y) : y;
     }
     __syncthreads();
     return r;

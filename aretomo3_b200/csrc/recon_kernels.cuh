@@ -247,7 +247,7 @@ __global__ void __launch_bounds__(512, RS < 2 ? 2 : 1) k_rweight(const float* __
 {
     extern __shared__ float2 fsm[];
     __shared__ float rsc[16];   // per row of the CTA: 1 / scale
-    const int pitch = plan.work;
+    const int pitch = fft_pitch(plan.work);
     float2* a = fsm;
     float2* b = fsm + (size_t)B * pitch;
     const int ys = blockIdx.y, pair0 = blockIdx.x * B;
@@ -262,7 +262,7 @@ __global__ void __launch_bounds__(512, RS < 2 ? 2 : 1) k_rweight(const float* __
         const float* s1 = srow + (size_t)(two ? t1 : t0) * tilt_stride;
         float2* aq = a + (size_t)q * pitch;
         staged_copy<4>(N, [&](int x) { return make_float2(__ldg(s0 + x) * w0, two ? __ldg(s1 + x) * w1 : 0.f); },
-                       [&](int x, float2 v) { aq[x] = v; });
+                       [&](int x, float2 v) { aq[fft_pad(x)] = v; });
     }
     __syncthreads();
     float2* r = fft_run<RS>(a, b, plan, nq, pitch, -1);
@@ -270,8 +270,8 @@ __global__ void __launch_bounds__(512, RS < 2 ? 2 : 1) k_rweight(const float* __
         float2* rq = r + (size_t)q * pitch;
         for (int k = threadIdx.x; k < N; k += blockDim.x) {
             const float h = __ldg(hhalf + (k <= N - k ? k : N - k));
-            const float2 v = rq[k];
-            rq[k] = make_float2(v.x * h, v.y * h);
+            const float2 v = rq[fft_pad(k)];
+            rq[fft_pad(k)] = make_float2(v.x * h, v.y * h);
         }
     }
     __syncthreads();
@@ -285,7 +285,8 @@ __global__ void __launch_bounds__(512, RS < 2 ? 2 : 1) k_rweight(const float* __
             const float2* rq = r2 + (size_t)q * pitch;
             float m = 0.f;
             for (int x = lane; x < N; x += 32) {
-                const float v = c ? rq[x].y : rq[x].x;
+                const float2 w2 = rq[fft_pad(x)];
+                const float v = c ? w2.y : w2.x;
                 if (v > kSentinelTest) m = fmaxf(m, fabsf(v));
             }
 #pragma unroll
@@ -307,7 +308,7 @@ __global__ void __launch_bounds__(512, RS < 2 ? 2 : 1) k_rweight(const float* __
         const float inv0 = std::is_same<ST, float>::value ? 1.f : rsc[2 * q];
         const float inv1 = std::is_same<ST, float>::value ? 1.f : rsc[2 * q + 1];
         for (int x = threadIdx.x; x < N; x += blockDim.x) {
-            const float2 v = rq[x];
+            const float2 v = rq[fft_pad(x)];
             Stor<ST>::st(d0 + x, v.x, inv0);
             low |= v.x <= kLowValue;
             if (two) {
@@ -1075,7 +1076,7 @@ __global__ void __launch_bounds__(512, RS < 2 ? 2 : 1) k_row_r2c(const float* __
                                                  float2* __restrict__ y)
 {
     extern __shared__ float2 fsm[];
-    const int pitch = plan.work;
+    const int pitch = fft_pitch(plan.work);
     float2* a = fsm;
     float2* b = fsm + (size_t)B * pitch;
     const int X2 = 2 * Nx, KX = Nx / 2 + 1;
@@ -1085,7 +1086,7 @@ __global__ void __launch_bounds__(512, RS < 2 ? 2 : 1) k_row_r2c(const float* __
         const float* g0 = g + ((size_t)ys * 2 * Nz + 2 * (pr0 + q)) * X2;
         float2* aq = a + (size_t)q * pitch;
         staged_copy<4>(X2, [&](int x) { return make_float2(__ldg(g0 + x), __ldg(g0 + X2 + x)); },
-                       [&](int x, float2 v) { aq[x] = v; });
+                       [&](int x, float2 v) { aq[fft_pad(x)] = v; });
     }
     __syncthreads();
     const float2* Zs = fft_run<RS>(a, b, plan, nq, pitch, -1);
@@ -1093,7 +1094,7 @@ __global__ void __launch_bounds__(512, RS < 2 ? 2 : 1) k_row_r2c(const float* __
         const float2* Z = Zs + (size_t)q * pitch;
         float2* y0 = y + ((size_t)ys * 2 * Nz + 2 * (pr0 + q)) * KX;
         for (int k = threadIdx.x; k < KX; k += blockDim.x) {
-            const float2 p = Z[k], qv = Z[k == 0 ? 0 : X2 - k];
+            const float2 p = Z[fft_pad(k)], qv = Z[fft_pad(k == 0 ? 0 : X2 - k)];
             // A = (p + conj q)/2 ; B = (p - conj q)/(2i) = -i (p - conj q)/2
             y0[k] = make_float2(0.5f * (p.x + qv.x), 0.5f * (p.y - qv.y));
             y0[KX + k] = make_float2(0.5f * (p.y + qv.y), -0.5f * (p.x - qv.x));
@@ -1127,7 +1128,7 @@ __global__ void __launch_bounds__(512, RS < 2 ? 2 : 1) k_zcrop(const float2* __r
                    },
                    [&](int idx, float2 v) {
                        const int Z = idx / CB, c = idx - Z * CB;
-                       a[(size_t)c * pitch + Z] = v;
+                       a[(size_t)c * pitch + fft_pad(Z)] = v;
                    });
     __syncthreads();
     float2* F = fft_run<RS>(a, b, p2, CB, pitch, -1);
@@ -1135,15 +1136,15 @@ __global__ void __launch_bounds__(512, RS < 2 ? 2 : 1) k_zcrop(const float2* __r
     for (int idx = threadIdx.x; idx < Nz * CB; idx += blockDim.x) {
         const int c = idx / Nz, kz = idx - c * Nz;
         const int src = kz <= Nz / 2 ? kz : kz + Nz;
-        const float2 v = F[(size_t)c * pitch + src];
-        G[(size_t)c * pitch + kz] = make_float2(v.x * norm, v.y * norm);
+        const float2 v = F[(size_t)c * pitch + fft_pad(src)];
+        G[(size_t)c * pitch + fft_pad(kz)] = make_float2(v.x * norm, v.y * norm);
     }
     __syncthreads();
     float2* H = fft_run<RS>(G, F, p1, CB, pitch, +1);
     float2* wsl = w + (size_t)ys * Nz * KX;
     for (int idx = threadIdx.x; idx < Nz * CB; idx += blockDim.x) {
         const int z = idx / CB, c = idx - z * CB;
-        if (c < nc) wsl[(size_t)z * KX + kx0 + c] = H[(size_t)c * pitch + z];
+        if (c < nc) wsl[(size_t)z * KX + kx0 + c] = H[(size_t)c * pitch + fft_pad(z)];
     }
 }
 
@@ -1163,7 +1164,7 @@ __global__ void __launch_bounds__(512, RS < 2 ? 2 : 1) k_x_c2r(const float2* __r
                                                int packed, float* __restrict__ vol, size_t vol_slice)
 {
     extern __shared__ float2 fsm[];
-    const int pitch = plan.work;
+    const int pitch = fft_pitch(plan.work);
     float2* a = fsm;
     float2* b = fsm + (size_t)B * pitch;
     const int KX = Nx / 2 + 1, H = Nx / 2;
@@ -1185,7 +1186,7 @@ __global__ void __launch_bounds__(512, RS < 2 ? 2 : 1) k_x_c2r(const float2* __r
                            if (!lo) { av.y = -av.y; bv.y = -bv.y; }
                            return make_float2(av.x - bv.y, av.y + bv.x);   // A + iB
                        },
-                       [&](int k, float2 v) { aq[k] = v; });
+                       [&](int k, float2 v) { aq[fft_pad(k)] = v; });
     }
     __syncthreads();
     const float2* rs = fft_run<RS>(a, b, plan, nq, pitch, +1);
@@ -1203,7 +1204,7 @@ __global__ void __launch_bounds__(512, RS < 2 ? 2 : 1) k_x_c2r(const float2* __r
         }
         float* o0 = vol + (size_t)ys * vol_slice + (size_t)(Nz - 1 - z0) * Nx;
         for (int x = threadIdx.x; x < Nx; x += blockDim.x) {
-            const float2 v = r[x];
+            const float2 v = r[fft_pad(x)];
             o0[x] = v.x + ((x & 1) ? oa : ea);
             if (two) o0[x - Nx] = v.y + ((x & 1) ? ob : eb);
         }
