@@ -37,7 +37,7 @@ def build_at3r(force: bool = False) -> str:
     if force or _newer(out, srcs):
         _run([NVCC, *ARCH, "-O3", "-lineinfo", "-std=c++17", "-shared", "-Xcompiler", "-fPIC",
               "-I", os.path.join(ROOT, "include"), "-o", out, os.path.join(CSRC, "at3r.cu"),
-              os.path.join(CSRC, "at3r_server.cpp"), "-ldl", "-lpthread"])
+              os.path.join(CSRC, "reproj.cu"), os.path.join(CSRC, "at3r_server.cpp"), "-ldl", "-lpthread"])
     return out
 
 

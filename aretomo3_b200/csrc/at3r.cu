@@ -597,6 +597,12 @@ at3r_status end_run(at3r_plan* p, cudaStream_t st)
 
 }  // namespace
 
+cudaMemPool_t at3r_device_pool(int dev)
+{
+    DevicePool* dp = device_pool(dev);
+    return dp ? dp->pool : nullptr;
+}
+
 extern "C" {
 
 void at3r_geom_init(at3r_geom* g, int method)

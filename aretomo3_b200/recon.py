@@ -83,6 +83,14 @@ _EXPORTS = {
     "at3r_server_in_use_bytes": (ctypes.c_size_t, [ctypes.c_void_p]),
     "at3r_server_destroy": (None, [ctypes.c_void_p]),
     "at3r_release_cached_memory": (None, []),
+    "at3r_reproj_range": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
+                                         ctypes.c_void_p]),
+    "at3r_reproj_device": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                          ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
+                                          ctypes.c_void_p, ctypes.c_void_p]),
+    "at3r_reproj_host": (ctypes.c_int, [ctypes.POINTER(ctypes.c_void_p), ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                        ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
+                                        ctypes.c_void_p, ctypes.c_void_p]),
     "at3r_status_str": (ctypes.c_char_p, [ctypes.c_int]),
     "at3r_last_error": (ctypes.c_char_p, []),
 }
@@ -397,6 +405,58 @@ def volume_xyz(vol, flip: bool = True, out=None, stream=None):
     s = stream if stream is not None else torch.cuda.current_stream(vol.device)
     _check(lib().at3r_volume_xyz(ctypes.c_void_p(vol.data_ptr()), nx, ny, nz, int(bool(flip)),
                                  ctypes.c_void_p(out.data_ptr()), ctypes.c_void_p(s.cuda_stream)))
+    return out
+
+
+class CCalcReproj:
+    """Mirror of ProjAlign::CCalcReproj (AreTomo/ProjAlign/CCalcReproj.cpp):
+    Setup(stack size, vol_z), then DoIt(frames, tilts, skip, proj_idx) returns
+    the re-projection of tilt proj_idx, [ny][nx] float32 (-1e30 where a ray
+    covers under 80 %).  skip: per-tilt flags as the caller keeps them (the
+    caller marks proj_idx itself, as CProjAlignMain::mCalcReproj does)."""
+
+    def Setup(self, tomo_stk_size, vol_z: int, nth_gpu: int = 0):
+        self.nx, self.ny, self.nt = (int(v) for v in tomo_stk_size)
+        self.vol_z = int(vol_z)
+
+    def DoIt(self, frames, tilts, skip, proj_idx: int, out: np.ndarray | None = None) -> np.ndarray:
+        tilts = np.ascontiguousarray(tilts, np.float32)
+        sk = None if skip is None else np.ascontiguousarray(skip, np.uint8)
+        if out is None:
+            out = np.empty((self.ny, self.nx), np.float32)
+        fr = (ctypes.c_void_p * self.nt)(*[np.ascontiguousarray(f, np.float32).ctypes.data if f is not None else None
+                                           for f in frames])
+        self._keep = frames
+        _check(lib().at3r_reproj_host(fr, self.nx, self.ny, self.nt, tilts.ctypes.data,
+                                      sk.ctypes.data if sk is not None else None, int(proj_idx), self.vol_z,
+                                      out.ctypes.data, None))
+        return out
+
+
+def reproj_range(tilts, proj_idx: int, skip=None):
+    """The tilt range [first, last] CCalcReproj::mFindProjRange picks."""
+    tilts = np.ascontiguousarray(tilts, np.float32)
+    sk = None if skip is None else np.ascontiguousarray(skip, np.uint8)
+    rng = np.zeros(2, np.int32)
+    _check(lib().at3r_reproj_range(tilts.ctypes.data, sk.ctypes.data if sk is not None else None, tilts.size,
+                                   int(proj_idx), rng.ctypes.data))
+    return int(rng[0]), int(rng[1])
+
+
+def reproj_device(proj, tilts, proj_idx: int, vol_z: int, skip=None, out=None, stream=None):
+    """Re-projection of tilt proj_idx from a torch CUDA tensor proj[T][ny][nx]."""
+    import torch
+    if not (proj.is_cuda and proj.dtype == torch.float32 and proj.is_contiguous()):
+        raise ValueError("proj must be a contiguous float32 CUDA tensor")
+    T, ny, nx = proj.shape
+    tilts = np.ascontiguousarray(tilts, np.float32)
+    sk = None if skip is None else np.ascontiguousarray(skip, np.uint8)
+    if out is None:
+        out = torch.empty((ny, nx), device=proj.device, dtype=torch.float32)
+    s = stream if stream is not None else torch.cuda.current_stream(proj.device)
+    _check(lib().at3r_reproj_device(ctypes.c_void_p(proj.data_ptr()), nx, ny, T, tilts.ctypes.data,
+                                    sk.ctypes.data if sk is not None else None, int(proj_idx), int(vol_z),
+                                    ctypes.c_void_p(out.data_ptr()), ctypes.c_void_p(s.cuda_stream)))
     return out
 
 

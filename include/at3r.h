@@ -163,6 +163,27 @@ void at3r_release_cached_memory(void);
 at3r_status at3r_run_host_xyz(at3r_plan* plan, const float* const* frames, float* vol_xyz, int flip, void* stream);
 at3r_status at3r_volume_xyz(const float* vol_xzy, int nx, int ny, int vol_z, int flip, float* vol_xyz, void* stream);
 
+/* Projection-alignment re-projection (replaces ProjAlign::CCalcReproj::DoIt,
+ * AreTomo/ProjAlign/CCalcReproj.cpp:36-58, with GReproj,
+ * AreTomo/ProjAlign/GReproj.cu): the image of tilt proj_idx re-projected from
+ * the nearby tilts.  The tilts [range[0], range[1]] that
+ * CCalcReproj::mFindProjRange picks (within 20.5 degrees, cos stretch <= 1.2,
+ * not skipped, at most 10; skip may be NULL) are back-projected, weighted by
+ * the cosine of their angle to tilt proj_idx, onto a (2 nx) x vol_z slice per
+ * row, and each slice is projected at tilt proj_idx with nearest-neighbour
+ * rays; reproj[ny][nx] holds the mean along each ray, -1e30 where a ray
+ * covers less than 80 % of its length.  As in the reference, the caller marks
+ * proj_idx itself in skip (CProjAlignMain::mCalcReproj).
+ * at3r_reproj_device: proj [n_tilts][ny][nx] and reproj on the device.
+ * at3r_reproj_host: host frames (only those of the range are copied) and a
+ * host reproj; returns when it is written. */
+at3r_status at3r_reproj_range(const float* tilts_deg, const unsigned char* skip, int n_tilts, int proj_idx,
+                              int* range);
+at3r_status at3r_reproj_device(const float* proj, int nx, int ny, int n_tilts, const float* tilts_deg,
+                               const unsigned char* skip, int proj_idx, int vol_z, float* reproj, void* stream);
+at3r_status at3r_reproj_host(const float* const* frames, int nx, int ny, int n_tilts, const float* tilts_deg,
+                             const unsigned char* skip, int proj_idx, int vol_z, float* reproj, void* stream);
+
 /* Slab autotuner: times the reconstruction of the leading rows (at most two
  * full-capacity slabs) with slab sizes from 4 slices up to the plan's
  * workspace capacity (doubling) on proj / vol (device buffers in the layouts

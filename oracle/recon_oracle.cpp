@@ -490,6 +490,103 @@ int sart_run(const float* frames, int nx, int ny, int T, const float* tilts, int
     return 0;
 }
 
+
+// ---------------------------------------------------------------------------
+// Projection-alignment re-projection (AreTomo/ProjAlign/CCalcReproj.cpp,
+// GReproj.cu).  FP32 throughout, in the reference kernels' operation order
+// (nvcc contracts a*b + c*d to fma(a, b, c*d) and x + y*z to fma(y, z, x)).
+// ---------------------------------------------------------------------------
+constexpr float kReprojD2R = 0.01745f;   // s_fD2R of GReproj.cu / CCalcReproj.cpp
+
+// CCalcReproj::mFindProjRange (CCalcReproj.cpp:66-119)
+void reproj_range(const float* tilts, const unsigned char* skip, int T, int proj, int* range)
+{
+    const float ref_range = 20.5f, ref_stretch = 1.20f;
+    const float a = tilts[proj];
+    const float cos_a = (float)std::cos((double)(a * kReprojD2R));
+    auto ok = [&](int i) {
+        if (skip && skip[i]) return false;
+        const float t = tilts[i];
+        if (std::fabs(a - t) > ref_range) return false;
+        const float stretch = (float)(std::cos((double)(t * kReprojD2R)) / cos_a);
+        return !(stretch > ref_stretch);
+    };
+    int start = -1, end = -1;
+    for (int i = 0; i < T; i++)
+        if (ok(i)) { start = i; break; }
+    for (int i = start; i >= 0 && i < T; i++)
+        if (ok(i)) end = i;
+    if (start < 0 || end < 0) {
+        const int sign = a > 0 ? 1 : -1;
+        start = proj - sign;
+        end = start;
+    }
+    if (end - start > 9) end = start + 9;
+    range[0] = start;
+    range[1] = end;
+}
+
+// GReproj mGBackProj + mGForProj for one row (GReproj.cu:22-110).  sino:
+// [T][nx] rows of the tilts in range; vol: scratch of (2 nx) x vz.
+void reproj_row(const float* const* rows, const float* tilts, const int* range, float proj_angle, int nx, int vz,
+                float* vol, float* out)
+{
+    const int VX = 2 * nx, VZ = vz;
+    const float cent = nx * 0.5f;
+    const int iend = nx - 1;
+    for (int z = 0; z < VZ; z++) {
+        const float fZ = z + 0.5f - VZ * 0.5f;
+        for (int x = 0; x < VX; x++) {
+            const float fX = x + 0.5f - VX * 0.5f;
+            float sum = 0.f, cnt = 0.f;
+            for (int i = range[0]; i <= range[1]; i++) {
+                const float w = cosf((proj_angle - tilts[i]) * kReprojD2R);
+                const float v = tilts[i] * kReprojD2R;
+                const float c = cosf(v), sn = sinf(v);
+                const float p = std::fmaf(fX, c, fZ * sn) + cent;
+                if (p < 0 || p > iend) continue;
+                float val = rows[i][(int)p];
+                if (val < -1e10f) val = -1e30f;
+                if (val < -1e20f) continue;
+                sum = std::fmaf(val * c, w, sum);
+                cnt += w;
+            }
+            vol[(size_t)z * VX + x] = cnt < 0.001f ? -1e30f : sum / cnt;
+        }
+    }
+    const double rad = 4.0 * std::atan(1.0) / 180.0;
+    const float c = (float)std::cos(rad * proj_angle), sn = (float)std::sin(rad * proj_angle);
+    const int L = (int)(VZ / c + 0.5f);
+    // a*b + c*d contracts to fma(a, b, c*d): the second product is rounded
+    const float tz = VZ * 0.5f - (L * 0.5f) * c;
+    constexpr int kT = 512;   // the reference's threads per ray
+    for (int u = 0; u < nx; u++) {
+        const float xp = u + 0.5f - nx * 0.5f;
+        const float tx = (VX * 0.5f + (L * 0.5f) * sn) + xp / c;
+        float part[kT];
+        int pcnt[kT];
+        for (int t = 0; t < kT; t++) {
+            float s = 0.f;
+            int n = 0;
+            for (int i = t; i < L; i += kT) {
+                const float fx = std::fmaf(-(float)i, sn, tx), fz = std::fmaf((float)i, c, tz);
+                if (fx < 0 || fx >= VX || fz < 0 || fz >= VZ) continue;
+                const float v = vol[(size_t)VX * (int)fz + (int)fx];
+                if (v <= -1e10f) continue;
+                s += v;
+                n += 1;
+            }
+            part[t] = s;
+            pcnt[t] = n;
+        }
+        for (int h = kT / 2; h > 0; h /= 2)
+            for (int t = 0; t < h; t++) {
+                part[t] += part[t + h];
+                pcnt[t] += pcnt[t + h];
+            }
+        out[u] = pcnt[0] < 0.8f * L ? -1e30f : part[0] / pcnt[0];
+    }
+}
 }  // namespace
 
 extern "C" {
@@ -568,6 +665,36 @@ int oracle_c2r_f64(const double* in_cplx, int n, double* out)
     std::vector<std::complex<double>> X(n / 2 + 1);
     for (int k = 0; k <= n / 2; k++) X[k] = {in_cplx[2 * k], in_cplx[2 * k + 1]};
     c2r<double>(X.data(), n, out, g_c2r_mode);
+    return 0;
+}
+
+int oracle_reproj_range(const float* tilts_deg, const unsigned char* skip, int n_tilts, int proj_idx, int* range)
+{
+    if (!tilts_deg || !range || n_tilts < 1 || proj_idx < 0 || proj_idx >= n_tilts) return -1;
+    reproj_range(tilts_deg, skip, n_tilts, proj_idx, range);
+    return 0;
+}
+
+int oracle_reproj_f32(const float* frames, int nx, int ny, int n_tilts, const float* tilts_deg,
+                      const unsigned char* skip, int proj_idx, int vol_z, float* out, int n_threads)
+{
+    if (!frames || !tilts_deg || !out || nx < 2 || ny < 1 || vol_z < 1 || proj_idx < 0 || proj_idx >= n_tilts)
+        return -1;
+    int range[2];
+    reproj_range(tilts_deg, skip, n_tilts, proj_idx, range);
+    if (range[0] < 0 || range[1] >= n_tilts) return -2;
+    const int nth = n_threads > 0 ? n_threads : 1;
+#pragma omp parallel num_threads(nth)
+    {
+        std::vector<float> vol((size_t)2 * nx * vol_z);
+        std::vector<const float*> rows(n_tilts);
+#pragma omp for schedule(dynamic, 1)
+        for (int y = 0; y < ny; y++) {
+            for (int t = 0; t < n_tilts; t++) rows[t] = frames + ((size_t)t * ny + y) * nx;
+            reproj_row(rows.data(), tilts_deg, range, tilts_deg[proj_idx], nx, vol_z, vol.data(),
+                       out + (size_t)y * nx);
+        }
+    }
     return 0;
 }
 

@@ -51,6 +51,17 @@ int oracle_sart_f32(const float* frames, int nx, int ny, int n_tilts, const floa
                     int vol_z, int start_tilt, int num_tilts, int iters, int subsets, double relax,
                     int y0, int y1, float* out, double* rfactor, int n_threads);
 
+/* Projection-alignment re-projection of tilt proj_idx
+ * (AreTomo/ProjAlign/CCalcReproj.cpp + GReproj.cu): for every row, the tilts
+ * of the range CCalcReproj::mFindProjRange picks (skip flags as the caller
+ * passes them; NULL = none) are back-projected onto a (2 nx) x vol_z slice
+ * and that slice is forward-projected at tilt proj_idx.  out: [ny][nx], -1e30
+ * where a ray covers less than 80 % of its length.  range: the tilt indices
+ * used, [first, last]. */
+int oracle_reproj_range(const float* tilts_deg, const unsigned char* skip, int n_tilts, int proj_idx, int* range);
+int oracle_reproj_f32(const float* frames, int nx, int ny, int n_tilts, const float* tilts_deg,
+                      const unsigned char* skip, int proj_idx, int vol_z, float* out, int n_threads);
+
 /* Components, for known-answer tests. */
 /* complex FFT of length n, interleaved re/im; sign -1 forward, +1 inverse, unnormalised */
 int oracle_fft_f64(const double* in, int n, int sign, double* out);

@@ -2,7 +2,9 @@
 # Test infrastructure only: compiles the reference's own CUDA Recon
 # (AreTomo3 AreTomo/Recon + the MaUtil/DataUtil/MrcUtil files it needs) for
 # sm_100a from the reference sources where they lie, plus this directory's
-# driver and stub, into oracle/_ref/ref_recon.  Nothing is copied out of the
+# driver and stub, into oracle/_ref/ref_recon; and its projection-alignment
+# re-projector (AreTomo/ProjAlign/GReproj + CCalcReproj) into
+# oracle/_ref/ref_reproj.  Nothing is copied out of the
 # reference tree; objects go to oracle/_ref/obj.
 set -euo pipefail
 REF=${AT3R_REFERENCE:-/root/reference}
@@ -37,3 +39,19 @@ g++ $CXXFLAGS -c "$HERE/ref_driver.cpp" -o "$OBJ/ref_driver.o"
 $NVCC -gencode arch=compute_100a,code=sm_100a -o "$OUT/ref_recon" "${objs[@]}" \
   "$OBJ/ref_stub.o" "$OBJ/ref_driver.o" -lcufft -lcurand -lcuda
 echo "built $OUT/ref_recon"
+
+# the projection-alignment re-projector (AreTomo/ProjAlign/GReproj.cu + CCalcReproj.cpp)
+rp=()
+for f in AreTomo/ProjAlign/GReproj; do
+  o="$OBJ/$(echo "$f" | tr / _).o"
+  [ "$o" -nt "$REF/$f.cu" ] || $NVCC $CUFLAGS -c "$REF/$f.cu" -o "$o"
+  rp+=("$o")
+done
+for f in AreTomo/ProjAlign/CCalcReproj; do
+  o="$OBJ/$(echo "$f" | tr / _).o"
+  [ "$o" -nt "$REF/$f.cpp" ] || g++ $CXXFLAGS -c "$REF/$f.cpp" -o "$o"
+  rp+=("$o")
+done
+g++ $CXXFLAGS -c "$HERE/ref_reproj_driver.cpp" -o "$OBJ/ref_reproj_driver.o"
+$NVCC -gencode arch=compute_100a,code=sm_100a -o "$OUT/ref_reproj" "${rp[@]}" "$OBJ/ref_reproj_driver.o"
+echo "built $OUT/ref_reproj"

@@ -8,7 +8,9 @@ seeded synthetic tilt series.  It needs a GPU, so it runs on a B200 box:
 and the resulting ``*.npz`` files are committed here.  Each fixture holds the
 input frames, the tilt angles, the reconstruction parameters and the volume
 exactly as ``CDoWbpRecon::DoIt`` / ``CDoSartRecon::DoIt`` returned it (one XZ
-slice per y, z flipped).
+slice per y, z flipped).  The ``reproj_*`` fixtures hold, in ``volume``, the
+re-projection ``CCalcReproj::DoIt`` returned (AreTomo/ProjAlign, built into
+oracle/_ref/ref_reproj), [ny][nx].
 """
 from __future__ import annotations
 
@@ -27,6 +29,7 @@ sys.path.insert(0, ROOT)
 from aretomo3_b200 import synth  # noqa: E402
 
 REF_BIN = os.path.join(ROOT, "oracle", "_ref", "ref_recon")
+REPROJ_BIN = os.path.join(ROOT, "oracle", "_ref", "ref_reproj")
 
 
 def small_phantom(seed, noise_kind=synth.NOISE_GAUSSIAN, noise_param=0.1):
@@ -56,6 +59,31 @@ def cases():
     c.append(dict(name="sart_1k_row", mode="sart", nx=1024, ny=1024, tilts=s["tilts"], vol_z=300,
                   phantom=s["phantom"], start=0, ntilts=61, iters=15, subsets=5, rows=(511, 512)))
     return c
+
+
+def reproj_cases():
+    """Re-projection fixtures: seeded series, the tilt re-projected is marked
+    skipped as CProjAlignMain::mCalcReproj does."""
+    t41 = synth.tilt_range(-60, 60, 3)
+    t31 = synth.tilt_range(-60, 60, 4) + np.float32(0.7)
+    c = []
+    c.append(dict(name="reproj_128_mid", nx=128, ny=6, tilts=t41, vol_z=48, phantom=small_phantom(31), proj=20))
+    c.append(dict(name="reproj_128_high", nx=128, ny=5, tilts=t41, vol_z=64, phantom=small_phantom(32), proj=3))
+    c.append(dict(name="reproj_97_end", nx=97, ny=4, tilts=t31, vol_z=37, phantom=small_phantom(33), proj=30))
+    return c
+
+
+def run_reference_reproj(frames, tilts, vol_z, proj):
+    with tempfile.TemporaryDirectory() as td:
+        fin, fout = os.path.join(td, "in.bin"), os.path.join(td, "out.bin")
+        write_input(fin, frames, tilts)
+        r = subprocess.run([REPROJ_BIN, fin, fout, str(vol_z), str(proj)], capture_output=True, text=True,
+                           check=True)
+        line = [ln for ln in r.stdout.splitlines() if ln.startswith("{")][-1]
+        with open(fout, "rb") as f:
+            nx, ny = np.fromfile(f, dtype=np.int32, count=2)
+            out = np.fromfile(f, dtype=np.float32).reshape(ny, nx)
+        return out, json.loads(line)
 
 
 def write_input(path, frames, tilts):
@@ -88,9 +116,13 @@ def run_reference(mode, frames, tilts, vol_z, start=0, ntilts=0, iters=0, subset
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", default=os.path.join(ROOT, "tests", "golden"))
+    ap.add_argument("--only", default="", help="comma-separated fixture names (default: all)")
     args = ap.parse_args()
     os.makedirs(args.out, exist_ok=True)
+    only = set(filter(None, args.only.split(",")))
     for c in cases():
+        if only and c["name"] not in only:
+            continue
         frames = synth.make_tilt_series(c["nx"], c["ny"], c["tilts"], c["vol_z"], c["phantom"])
         if "rows" in c:
             r0, r1 = c["rows"]
@@ -103,6 +135,17 @@ def main():
                             tilts=np.asarray(c["tilts"], np.float32), volume=vol,
                             meta=json.dumps(meta))
         print(c["name"], vol.shape, info)
+    for c in reproj_cases():
+        if only and c["name"] not in only:
+            continue
+        frames = synth.make_tilt_series(c["nx"], c["ny"], c["tilts"], c["vol_z"], c["phantom"])
+        out, info = run_reference_reproj(frames, c["tilts"], c["vol_z"], c["proj"])
+        meta = {k: v for k, v in c.items() if k not in ("tilts", "phantom")}
+        meta["mode"] = "reproj"
+        meta["reference_run"] = info
+        np.savez_compressed(os.path.join(args.out, c["name"] + ".npz"), frames=frames,
+                            tilts=np.asarray(c["tilts"], np.float32), volume=out, meta=json.dumps(meta))
+        print(c["name"], out.shape, info)
 
 
 if __name__ == "__main__":

@@ -24,7 +24,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, HERE)
 import gen_golden  # noqa: E402
-from gen_golden import ROOT, run_reference  # noqa: E402
+from gen_golden import ROOT, run_reference  # noqa: E402, F401
 
 from aretomo3_b200 import recon, synth  # noqa: E402
 
@@ -75,5 +75,39 @@ def main():
                           "speedup": info["seconds"] / t_ours, "rel_l2_vs_reference": rel}), flush=True)
 
 
+def reproj_workloads():
+    """The projection-alignment re-projector on a 1024 x 1024 x 61 binned
+    stack, alignment thickness 300, at a low and a high tilt."""
+    s = synth.sart_1k()
+    for proj in (30, 5):
+        yield dict(s, name=f"reproj_1k_t{proj}", proj=proj)
+
+
+def main_reproj():
+    if not os.path.exists(gen_golden.REPROJ_BIN):
+        print(json.dumps({"unavailable": "oracle/_ref/ref_reproj not built"}))
+        return
+    for c in reproj_workloads():
+        frames = synth.make_tilt_series(c["nx"], c["ny"], c["tilts"], c["vol_z"], c["phantom"])
+        ref, info = gen_golden.run_reference_reproj(frames, c["tilts"], c["vol_z"], c["proj"])
+        T, ny, nx = frames.shape
+        skip = np.zeros(T, np.uint8)
+        skip[c["proj"]] = 1
+        calc = recon.CCalcReproj()
+        calc.Setup((nx, ny, T), c["vol_z"])
+        fr = [frames[t] for t in range(T)]
+        calc.DoIt(fr, c["tilts"], skip, c["proj"])   # warm-up
+        ts = []
+        for _ in range(3):
+            t = time.perf_counter()
+            got = calc.DoIt(fr, c["tilts"], skip, c["proj"])
+            ts.append(time.perf_counter() - t)
+        t_ours = float(np.median(ts))
+        print(json.dumps({"workload": c["name"], "shape": [T, ny, nx], "vol_z": c["vol_z"], "proj": c["proj"],
+                          "reference_s": info["seconds"], "ours_s": t_ours, "speedup": info["seconds"] / t_ours,
+                          "bit_identical": bool(np.array_equal(got, ref))}), flush=True)
+
+
 if __name__ == "__main__":
     main()
+    main_reproj()

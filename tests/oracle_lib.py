@@ -73,3 +73,28 @@ def load_golden(name):
     import json
     z = np.load(os.path.join(ROOT, "tests", "golden", name + ".npz"))
     return z["frames"], z["tilts"], z["volume"], json.loads(str(z["meta"]))
+
+
+def reproj_range(tilts, proj_idx, skip=None):
+    tilts = np.ascontiguousarray(tilts, np.float32)
+    sk = None if skip is None else np.ascontiguousarray(skip, np.uint8)
+    rng = np.zeros(2, np.int32)
+    rc = lib().oracle_reproj_range(_p(tilts), _p(sk) if sk is not None else None, tilts.size, int(proj_idx),
+                                   _p(rng))
+    if rc != 0:
+        raise ValueError(f"oracle reproj range rc={rc}")
+    return int(rng[0]), int(rng[1])
+
+
+def reproj(frames, tilts, proj_idx, vol_z, skip=None, threads=os.cpu_count()):
+    """Re-projection of tilt proj_idx (FP32 restatement of CCalcReproj + GReproj)."""
+    frames = np.ascontiguousarray(frames, np.float32)
+    tilts = np.ascontiguousarray(tilts, np.float32)
+    t, ny, nx = frames.shape
+    sk = None if skip is None else np.ascontiguousarray(skip, np.uint8)
+    out = np.zeros((ny, nx), np.float32)
+    rc = lib().oracle_reproj_f32(_p(frames), nx, ny, t, _p(tilts), _p(sk) if sk is not None else None,
+                                 int(proj_idx), int(vol_z), _p(out), threads)
+    if rc != 0:
+        raise ValueError(f"oracle reproj rc={rc}")
+    return out

@@ -74,3 +74,18 @@ def test_estimate_bytes_without_gpu():
     big = recon.estimate_bytes(4096, 4096, tilts, 1200, method=recon.SART, storage=recon.STORE_F16)
     assert big > 2 * 8 * 4096 * 1200 * 4
     assert recon.estimate_bytes(0, 64, tilts, 64) == 0
+
+
+def test_reproj_range_matches_oracle_without_gpu():
+    """The product's tilt-range choice (CCalcReproj::mFindProjRange) equals
+    the oracle's on random tilt sets, skip flags and projection indices."""
+    import oracle_lib as ol
+    from aretomo3_b200 import recon
+    rng = np.random.default_rng(0)
+    for _ in range(200):
+        T = int(rng.integers(3, 70))
+        tilts = np.sort(rng.uniform(rng.uniform(-70, -20), rng.uniform(20, 70), T)).astype(np.float32)
+        p = int(rng.integers(0, T))
+        skip = (rng.random(T) < 0.15).astype(np.uint8)
+        skip[p] = 1
+        assert recon.reproj_range(tilts, p, skip) == ol.reproj_range(tilts, p, skip)
