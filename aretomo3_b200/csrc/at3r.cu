@@ -952,6 +952,20 @@ void stage_release(char* s)
 }
 
 // Borrows a staging set for this run; the caller returns it with stage_return.
+// Consecutive pieces whose source and destination both continue where the
+// previous one ended, merged into one (fewer, larger copies).
+std::vector<Piece> merge_pieces(const std::vector<Piece>& in)
+{
+    std::vector<Piece> out;
+    for (const Piece& pc : in) {
+        if (!out.empty() && out.back().dst + out.back().bytes == pc.dst && out.back().src + out.back().bytes == pc.src)
+            out.back().bytes += pc.bytes;
+        else
+            out.push_back(pc);
+    }
+    return out;
+}
+
 at3r_status ensure_stage(at3r_plan* p)
 {
     char* s = stage_acquire();
@@ -994,11 +1008,14 @@ at3r_status stage_in(at3r_plan* p, const std::vector<Piece>& pieces, int& slot)
             o += pc.bytes;
         }
         parallel_copy(host);
+        std::vector<Piece> dev;
         o = 0;
         for (const Piece& pc : chunk) {
-            AT3R_CUDA(cudaMemcpyAsync(pc.dst, st + o, pc.bytes, cudaMemcpyHostToDevice, p->s_copy_in));
+            dev.push_back({pc.dst, st + o, pc.bytes});
             o += pc.bytes;
         }
+        for (const Piece& pc : merge_pieces(dev))
+            AT3R_CUDA(cudaMemcpyAsync(pc.dst, pc.src, pc.bytes, cudaMemcpyHostToDevice, p->s_copy_in));
         AT3R_CUDA(cudaEventRecord(p->ev_stage[slot], p->s_copy_in));
         slot ^= 1;
         chunk.clear();
@@ -1042,11 +1059,14 @@ at3r_status stage_out(at3r_plan* p, const std::vector<Piece>& pieces)
         char* st = p->h_stage_out[slot];
         Pending d{slot, {}};
         size_t o = 0;
+        std::vector<Piece> dev;
         for (const Piece& pc : chunk) {
-            AT3R_CUDA(cudaMemcpyAsync(st + o, pc.src, pc.bytes, cudaMemcpyDeviceToHost, p->s_copy_out));
+            dev.push_back({st + o, pc.src, pc.bytes});
             d.host.push_back({pc.dst, st + o, pc.bytes});
             o += pc.bytes;
         }
+        for (const Piece& pc : merge_pieces(dev))
+            AT3R_CUDA(cudaMemcpyAsync(pc.dst, pc.src, pc.bytes, cudaMemcpyDeviceToHost, p->s_copy_out));
         AT3R_CUDA(cudaEventRecord(p->ev_stage[2 + slot], p->s_copy_out));
         pend.push_back(std::move(d));
         slot ^= 1;
@@ -1171,9 +1191,14 @@ at3r_status run_host_body(at3r_plan* p, const float* const* frames, float* const
                                         sizeof(float) * (size_t)n * p->Nx, p->Nz, cudaMemcpyDeviceToHost,
                                         p->s_copy_out));
         } else {
+            // frames that sit back to back in host memory go out as one copy
+            std::vector<Piece> pc;
             for (int j = 0; j < n; j++)
-                AT3R_CUDA(cudaMemcpyAsync(vol_frames[y0 + j], p->d_vol_slab[b] + (size_t)j * slice,
-                                          sizeof(float) * slice, cudaMemcpyDeviceToHost, p->s_copy_out));
+                pc.push_back({reinterpret_cast<char*>(vol_frames[y0 + j]),
+                              reinterpret_cast<const char*>(p->d_vol_slab[b] + (size_t)j * slice),
+                              sizeof(float) * slice});
+            for (const Piece& m : merge_pieces(pc))
+                AT3R_CUDA(cudaMemcpyAsync(m.dst, m.src, m.bytes, cudaMemcpyDeviceToHost, p->s_copy_out));
         }
         AT3R_CUDA(cudaEventRecord(p->ev[4 + b], p->s_copy_out));
     }
