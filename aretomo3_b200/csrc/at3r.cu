@@ -273,6 +273,17 @@ struct at3r_plan {
     void* d_filt = nullptr;
     float* d_g2 = nullptr;    // also holds the cropped spectrum w
     float2* d_y = nullptr;
+    // WBP: a second workspace and stream, so that alternate slabs overlap
+    // (one slab's kernel tails fill with the next slab's kernels)
+    struct WbpLane {
+        void* filt = nullptr;
+        float* scale = nullptr;
+        int* flags = nullptr;
+        float* g2 = nullptr;
+        float2* y = nullptr;
+    } lane2;
+    cudaStream_t s_lane2 = nullptr;
+    cudaEvent_t ev_lane[2] = {};
     HostFft fN, f2x, f2z, fz, fx;
     int zcrop_cb = 4, zcrop_pitch = 0;
     int b_rweight = 1, b_row = 1, b_xc2r = 1;   // sequences per CTA of the row FFT kernels
@@ -464,16 +475,22 @@ at3r_status tend(at3r_plan* p, cudaStream_t st, int kind, double bytes, double u
 // slab's first output slice.
 template <typename ST, typename VT>
 at3r_status run_slab_t(at3r_plan* p, const float* proj, size_t tilt_stride, int proj_y0, int S, float* vol,
-                       cudaStream_t st)
+                       cudaStream_t st, int lane)
 {
+    // WBP slabs on the second lane use its workspace
+    int* const flags = lane ? p->lane2.flags : p->d_flags;
+    float* const scale = lane ? p->lane2.scale : p->d_scale;
+    void* const filt_ws = lane ? p->lane2.filt : p->d_filt;
+    float* const g2 = lane ? p->lane2.g2 : p->d_g2;
+    float2* const yws = lane ? p->lane2.y : p->d_y;
     ST* raw = static_cast<ST*>(p->d_raw);
     ST* dif = static_cast<ST*>(p->d_diff);
-    ST* filt = static_cast<ST*>(p->d_filt);
+    ST* filt = static_cast<ST*>(filt_ws);
     const double es = (double)sizeof(ST), vs = std::is_same<VT, float>::value ? 4.0 : 2.0;
     const int T = p->T, N = p->N, Nx = p->Nx, Nz = p->Nz, KX = p->KX;
     const double f4 = 4.0, vox = (double)S * Nx * Nz;
     const int SG = (S + SB - 1) / SB;   // slice groups: each thread carries SB slices
-    AT3R_CUDA(cudaMemsetAsync(p->d_flags, 0, sizeof(int) * S, st));
+    AT3R_CUDA(cudaMemsetAsync(flags, 0, sizeof(int) * S, st));
     if (p->g.method == AT3R_SART) {
         TB(p, st);
         k_gather_weight<ST><<<dim3(T, S), 256, 0, st>>>(proj, tilt_stride, p->nx, proj_y0, p->d_cs, T, N, Nz, raw,
@@ -528,13 +545,13 @@ at3r_status run_slab_t(at3r_plan* p, const float* proj, size_t tilt_stride, int 
         k_rweight<ST, decltype(R)::value><<<dim3(((T + 1) / 2 + p->b_rweight - 1) / p->b_rweight, S), 512,
                                             p->smem_rweight, st>>>(proj, tilt_stride, p->nx, proj_y0, p->d_cs, T, N,
                                                                    Nz, p->d_h, p->fN.plan, p->b_rweight, filt,
-                                                                   p->d_scale, p->d_flags);
+                                                                   scale, flags);
     });
     TE(p, st, KK_RWEIGHT, (f4 + es) * S * T * N, (double)S * T * N);
     BpArgs a{};
-    a.sino = filt; a.scale = p->d_scale; a.shadow = nullptr; a.T = T; a.N = N; a.t0 = 0; a.t1 = T; a.cs = p->d_cs;
-    a.GX = 2 * Nx; a.GZ = 2 * Nz; a.S = S; a.relax = 1.f; a.out = p->d_g2; a.out_slice = (size_t)4 * Nx * Nz;
-    a.ww = p->bp_ww_wbp; a.flags = p->d_flags; a.low_bit = kFlagRawLow;
+    a.sino = filt; a.scale = scale; a.shadow = nullptr; a.T = T; a.N = N; a.t0 = 0; a.t1 = T; a.cs = p->d_cs;
+    a.GX = 2 * Nx; a.GZ = 2 * Nz; a.S = S; a.relax = 1.f; a.out = g2; a.out_slice = (size_t)4 * Nx * Nz;
+    a.ww = p->bp_ww_wbp; a.flags = flags; a.low_bit = kFlagRawLow;
     const dim3 bgrid((2 * Nx + BP_TX - 1) / BP_TX, (2 * Nz + BP_TZ - 1) / BP_TZ, SG);
     TB(p, st);
     k_bp<1, ST, float, false><<<bgrid, BP_THREADS, bp_smem(T, a.ww), st>>>(a);
@@ -542,15 +559,15 @@ at3r_status run_slab_t(at3r_plan* p, const float* proj, size_t tilt_stride, int 
     TB(p, st);
     dispatch_rs(p->f2x.rs, [&](auto R) {
         k_row_r2c<decltype(R)::value><<<dim3((Nz + p->b_row - 1) / p->b_row, S), 512, p->smem_row, st>>>(
-            p->d_g2, Nx, Nz, p->f2x.plan, p->b_row, p->d_y);
+            g2, Nx, Nz, p->f2x.plan, p->b_row, yws);
     });
     TE(p, st, KK_ROW_R2C, f4 * 4 * vox + 8.0 * S * 2 * Nz * KX, 4 * vox);
     const float norm = (float)(1.0 / (2.0 * Nx) / (2.0 * Nz));
-    float2* w = reinterpret_cast<float2*>(p->d_g2);
+    float2* w = reinterpret_cast<float2*>(g2);
     TB(p, st);
     dispatch_rs(p->rs_zcrop, [&](auto R) {
         k_zcrop<decltype(R)::value><<<dim3((KX + p->zcrop_cb - 1) / p->zcrop_cb, S), 512, p->smem_zcrop, st>>>(
-            p->d_y, Nx, Nz, p->zcrop_cb, p->zcrop_pitch, p->f2z.plan, p->fz.plan, norm, w);
+            yws, Nx, Nz, p->zcrop_cb, p->zcrop_pitch, p->f2z.plan, p->fz.plan, norm, w);
     });
     TE(p, st, KK_ZCROP, 8.0 * S * 3 * Nz * KX, (double)S * 2 * Nz * KX);
     TB(p, st);
@@ -563,14 +580,30 @@ at3r_status run_slab_t(at3r_plan* p, const float* proj, size_t tilt_stride, int 
 }
 
 at3r_status run_slab(at3r_plan* p, const float* proj, size_t tilt_stride, int proj_y0, int S, float* vol,
-                     cudaStream_t st)
+                     cudaStream_t st, int lane = 0)
 {
     switch (p->g.storage) {
-        case AT3R_STORE_F16: return run_slab_t<__half, __half>(p, proj, tilt_stride, proj_y0, S, vol, st);
+        case AT3R_STORE_F16: return run_slab_t<__half, __half>(p, proj, tilt_stride, proj_y0, S, vol, st, lane);
         case AT3R_STORE_BF16:
-            return run_slab_t<__nv_bfloat16, __nv_bfloat16>(p, proj, tilt_stride, proj_y0, S, vol, st);
-        default: return run_slab_t<float, float>(p, proj, tilt_stride, proj_y0, S, vol, st);
+            return run_slab_t<__nv_bfloat16, __nv_bfloat16>(p, proj, tilt_stride, proj_y0, S, vol, st, lane);
+        default: return run_slab_t<float, float>(p, proj, tilt_stride, proj_y0, S, vol, st, lane);
     }
+}
+
+// The second WBP lane: allocated on first use (a run of two or more slabs).
+at3r_status ensure_lane2(at3r_plan* p)
+{
+    if (p->s_lane2) return AT3R_OK;
+    const size_t S = p->slab, T = p->T, N = p->N, Nx = p->Nx, Nz = p->Nz, KX = p->KX;
+    at3r_status rc;
+    if ((rc = dalloc_bytes(p, &p->lane2.filt, S * T * N * p->esz))) return rc;
+    if (p->g.storage != AT3R_STORE_F32 && (rc = dalloc(p, &p->lane2.scale, S * T))) return rc;
+    if ((rc = dalloc(p, &p->lane2.flags, S))) return rc;
+    if ((rc = dalloc(p, &p->lane2.g2, S * 4 * Nx * Nz))) return rc;
+    if ((rc = dalloc(p, &p->lane2.y, S * 2 * Nz * KX))) return rc;
+    for (cudaEvent_t& e : p->ev_lane) AT3R_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    AT3R_CUDA(cudaStreamCreateWithFlags(&p->s_lane2, cudaStreamNonBlocking));
+    return AT3R_OK;
 }
 
 at3r_status begin_run(at3r_plan* p, cudaStream_t st)
@@ -665,8 +698,9 @@ size_t at3r_plan_estimate_bytes(const at3r_geom* g)
     size_t work;
     if (g->method == AT3R_SART)
         work = (slab + 3) * (2 * T * N * esz + 4 * Nx * Nz + (esz < 4 ? 2 * Nx * Nz + T * 4 : 0)) + slab * 8;
-    else
-        work = slab * (T * N * esz + 16 * Nx * Nz + 2 * Nz * KX * sizeof(float2) + (esz < 4 ? T * 4 : 0) + 4);
+    else   // two lanes of slab workspace when the series has more than one slab (device path)
+        work = (slab < (size_t)g->ny ? 2 : 1) *
+               slab * (T * N * esz + 16 * Nx * Nz + 2 * Nz * KX * sizeof(float2) + (esz < 4 ? T * 4 : 0) + 4);
     const size_t host_path = 2 * (T * slab * nx + slab * Nx * Nz) * sizeof(float);
     return work + host_path + tables + T * 8 + (1 << 20);
 }
@@ -835,6 +869,11 @@ void at3r_plan_destroy(at3r_plan* p)
                       (void*)p->d_flags, (void*)p->d_rf, (void*)p->d_h, (void*)p->d_filt, (void*)p->d_g2,
                       (void*)p->d_y})
         dfree(p, ptr);
+    for (void* ptr : {p->lane2.filt, (void*)p->lane2.scale, (void*)p->lane2.flags, (void*)p->lane2.g2,
+                      (void*)p->lane2.y})
+        dfree(p, ptr);
+    if (p->s_lane2) cudaStreamDestroy(p->s_lane2);
+    for (cudaEvent_t& e : p->ev_lane) if (e) cudaEventDestroy(e);
     for (HostFft* f : {&p->fN, &p->f2x, &p->f2z, &p->fz, &p->fx}) dfree(p, f->d_tables);
     for (int i = 0; i < 2; i++) { dfree(p, p->d_proj_slab[i]); dfree(p, p->d_vol_slab[i]); dfree(p, p->d_xyz_slab[i]); }
     if (p->s_copy_in) cudaStreamDestroy(p->s_copy_in);
@@ -852,9 +891,21 @@ at3r_status at3r_run_device(at3r_plan* p, const float* proj, float* vol, void* s
     at3r_status rc;
     if ((rc = begin_run(p, st))) return rc;
     const size_t tilt_stride = (size_t)p->ny * p->nx;
-    for (int y0 = 0; y0 < p->ny; y0 += p->slab) {
-        const int S = std::min(p->slab, p->ny - y0);
-        if ((rc = run_slab(p, proj, tilt_stride, y0, S, vol + (size_t)y0 * p->Nx * p->Nz, st))) return rc;
+    const bool two = p->g.method == AT3R_WBP && p->ny > p->slab && ensure_lane2(p) == AT3R_OK;
+    if (two) {
+        // alternate slabs on two streams: fork from st, join back at the end
+        AT3R_CUDA(cudaEventRecord(p->ev_lane[0], st));
+        AT3R_CUDA(cudaStreamWaitEvent(p->s_lane2, p->ev_lane[0], 0));
+    }
+    for (int k = 0, y0 = 0; y0 < p->ny; y0 += p->slab, k++) {
+        const int S = std::min(p->slab, p->ny - y0), lane = two ? (k & 1) : 0;
+        if ((rc = run_slab(p, proj, tilt_stride, y0, S, vol + (size_t)y0 * p->Nx * p->Nz, lane ? p->s_lane2 : st,
+                           lane)))
+            return rc;
+    }
+    if (two) {
+        AT3R_CUDA(cudaEventRecord(p->ev_lane[1], p->s_lane2));
+        AT3R_CUDA(cudaStreamWaitEvent(st, p->ev_lane[1], 0));
     }
     return end_run(p, st);
 }
@@ -1166,18 +1217,23 @@ at3r_status run_host_body(at3r_plan* p, const float* const* frames, float* const
         return AT3R_OK;
     };
     if ((rc = copy_in(0))) return rc;
+    // one compute stream here: with slabs overlapping on two streams the
+    // first slab would finish later, and the copies out (the bound of this
+    // path) would start later
     for (int k = 0; k < nslab; k++) {
         const int b = k & 1, y0 = k * p->slab, n = std::min(p->slab, p->ny - y0);
+        const int lane = 0;
+        cudaStream_t cs = st;
         if (k + 1 < nslab && (rc = copy_in(k + 1))) return rc;
-        AT3R_CUDA(cudaStreamWaitEvent(st, p->ev[b], 0));
-        if (k >= 2) AT3R_CUDA(cudaStreamWaitEvent(st, p->ev[4 + b], 0));
-        if ((rc = run_slab(p, p->d_proj_slab[b], S * nx, 0, n, p->d_vol_slab[b], st))) return rc;
+        AT3R_CUDA(cudaStreamWaitEvent(cs, p->ev[b], 0));
+        if (k >= 2) AT3R_CUDA(cudaStreamWaitEvent(cs, p->ev[4 + b], 0));
+        if ((rc = run_slab(p, p->d_proj_slab[b], S * nx, 0, n, p->d_vol_slab[b], cs, lane))) return rc;
         if (vol_xyz) {
-            k_flip_rows<<<dim3(p->Nz, n), 256, 0, st>>>(p->d_vol_slab[b], p->d_xyz_slab[b], p->Nz, p->Nx, flip,
+            k_flip_rows<<<dim3(p->Nz, n), 256, 0, cs>>>(p->d_vol_slab[b], p->d_xyz_slab[b], p->Nz, p->Nx, flip,
                                                         (size_t)n * p->Nx);
             p->launches++;
         }
-        AT3R_CUDA(cudaEventRecord(p->ev[2 + b], st));
+        AT3R_CUDA(cudaEventRecord(p->ev[2 + b], cs));
         if (!out_pinned) {
             // slab k computes while the host drains slab k - 1
             if (k >= 1 && (rc = drain_out(k - 1))) return rc;
