@@ -531,26 +531,38 @@ __global__ void __launch_bounds__(BP_THREADS, 3) k_bp(BpArgs p)
         // all its loads of the row before its first store, so a warp waits for
         // the L2 once per row rather than once per load
         constexpr int NW = BP_THREADS / 32, KS = (BP_WW + 31) / 32;
+        // rows (slice q, tilt t) of the chunk, warp `warp` takes every NW-th;
+        // q and t advance without a division
+        int q = warp / nc, t = warp - (warp / nc) * nc;
         for (int row = warp; row < ns * nc; row += NW) {
-            const int q = row / nc, t = row - q * nc;
             const int x0 = ws[t];
             const size_t row_id = (size_t)(ysA + q) * p.T + c0 + t;
-            const ST* src = reinterpret_cast<const ST*>(p.sino) + row_id * p.N;
             const float sc = std::is_same<ST, float>::value ? 1.f : __ldg(p.scale + row_id);
-            float2* dst = pw + q * BP_PSLAB + t * BP_WW;
+            const ST* src = reinterpret_cast<const ST*>(p.sino) + row_id * p.N + x0 + lane;
+            float2* dst = pw + q * BP_PSLAB + t * BP_WW + lane;
             float va[KS], vb[KS];
+            if (x0 >= 0 && x0 + p.ww + 1 <= p.N) {
+                // the whole window lies on the detector (warp-uniform)
 #pragma unroll
-            for (int u = 0; u < KS; u++) {
-                const int k = lane + 32 * u, x = x0 + k;
-                const bool kv = k < p.ww;
-                va[u] = (kv && x >= 0 && x < p.N) ? Stor<ST>::ld(src + x, sc) : 0.f;
-                vb[u] = (kv && x + 1 >= 0 && x + 1 < p.N) ? Stor<ST>::ld(src + x + 1, sc) : 0.f;
+                for (int u = 0; u < KS; u++) {
+                    const bool kv = lane + 32 * u < p.ww;
+                    va[u] = kv ? Stor<ST>::ld(src + 32 * u, sc) : 0.f;
+                    vb[u] = kv ? Stor<ST>::ld(src + 32 * u + 1, sc) : 0.f;
+                }
+            } else {
+#pragma unroll
+                for (int u = 0; u < KS; u++) {
+                    const int k = lane + 32 * u, x = x0 + k;
+                    const bool kv = k < p.ww;
+                    va[u] = (kv && x >= 0 && x < p.N) ? Stor<ST>::ld(src + 32 * u, sc) : 0.f;
+                    vb[u] = (kv && x + 1 >= 0 && x + 1 < p.N) ? Stor<ST>::ld(src + 32 * u + 1, sc) : 0.f;
+                }
             }
 #pragma unroll
-            for (int u = 0; u < KS; u++) {
-                const int k = lane + 32 * u;
-                if (k < p.ww) dst[k] = make_float2(va[u], vb[u]);
-            }
+            for (int u = 0; u < KS; u++)
+                if (lane + 32 * u < p.ww) dst[32 * u] = make_float2(va[u], vb[u]);
+            t += NW;
+            while (t >= nc) { t -= nc; q++; }
         }
         __syncthreads();
         return inside != 0;
