@@ -139,6 +139,15 @@ struct Quad<__nv_bfloat16> {
     }
 };
 
+// acc + h in one mixed-precision add (FP16 operand, FP32 result); the same
+// value as converting h to FP32 (exact) and adding.
+__device__ __forceinline__ float add_f32_f16(float acc, __half h)
+{
+    float r;
+    asm("add.rn.f32.f16 %0, %1, %2;" : "=f"(r) : "h"(__half_as_ushort(h)), "f"(acc));
+    return r;
+}
+
 __device__ __forceinline__ float comp(const float4& v, int q)
 {
     return q == 0 ? v.x : q == 1 ? v.y : q == 2 ? v.z : v.w;
@@ -855,7 +864,7 @@ __global__ void __launch_bounds__(256) k_fp_diff(const float* __restrict__ vol, 
             const float w00 = ux * uz, w10 = wx * uz, w01 = ux * wz, w11 = wx * wz;
             if constexpr (std::is_same<VT, __half>::value) {
                 // FP16 shadow: the sample value of two slices per half2
-                // instruction, converted once and summed in FP32
+                // instruction, added to the FP32 sums by mixed-precision adds
                 const uint2 b00 = __ldg(reinterpret_cast<const uint2*>(g0 + o));
                 const uint2 b10 = __ldg(reinterpret_cast<const uint2*>(g0 + o + 1));
                 const uint2 b01 = __ldg(reinterpret_cast<const uint2*>(g1 + o));
@@ -870,11 +879,10 @@ __global__ void __launch_bounds__(256) k_fp_diff(const float* __restrict__ vol, 
                 hi = __hfma2(h01, from_bits<__half2>(b01.y), hi);
                 lo = __hfma2(h11, from_bits<__half2>(b11.x), lo);
                 hi = __hfma2(h11, from_bits<__half2>(b11.y), hi);
-                const float2 flo = __half22float2(lo), fhi = __half22float2(hi);
-                fSum[0] += flo.x;
-                fSum[1] += flo.y;
-                fSum[2] += fhi.x;
-                fSum[3] += fhi.y;
+                fSum[0] = add_f32_f16(fSum[0], __low2half(lo));
+                fSum[1] = add_f32_f16(fSum[1], __high2half(lo));
+                fSum[2] = add_f32_f16(fSum[2], __low2half(hi));
+                fSum[3] = add_f32_f16(fSum[3], __high2half(hi));
                 continue;
             }
             const float4 a00 = Quad<VT>::ld(g0 + o), a10 = Quad<VT>::ld(g0 + o + 1);
