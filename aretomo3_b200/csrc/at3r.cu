@@ -891,7 +891,8 @@ at3r_status at3r_run_device(at3r_plan* p, const float* proj, float* vol, void* s
     at3r_status rc;
     if ((rc = begin_run(p, st))) return rc;
     const size_t tilt_stride = (size_t)p->ny * p->nx;
-    const bool two = p->g.method == AT3R_WBP && p->ny > p->slab && ensure_lane2(p) == AT3R_OK;
+    // (one lane while per-kernel timing is on: overlapping kernels would time each other)
+    const bool two = p->g.method == AT3R_WBP && !p->timing && p->ny > p->slab && ensure_lane2(p) == AT3R_OK;
     if (two) {
         // alternate slabs on two streams: fork from st, join back at the end
         AT3R_CUDA(cudaEventRecord(p->ev_lane[0], st));
