@@ -31,13 +31,27 @@ def _run(cmd: list[str]) -> None:
 
 
 def build_at3r(force: bool = False) -> str:
+    """Compiles the CUDA / C++ sources to objects in parallel (csrc/_build/),
+    then links libat3r.so."""
     out = os.path.join(PKG, "libat3r.so")
     srcs = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cu", ".cuh", ".h", ".cpp"))]
     srcs.append(os.path.join(ROOT, "include", "at3r.h"))
-    if force or _newer(out, srcs):
-        _run([NVCC, *ARCH, "-O3", "-lineinfo", "-std=c++17", "-shared", "-Xcompiler", "-fPIC",
-              "-I", os.path.join(ROOT, "include"), "-o", out, os.path.join(CSRC, "at3r.cu"),
-              os.path.join(CSRC, "reproj.cu"), os.path.join(CSRC, "at3r_server.cpp"), "-ldl", "-lpthread"])
+    if not (force or _newer(out, srcs)):
+        return out
+    units = ["at3r.cu", "reproj.cu", "stack.cu", "at3r_server.cpp"]
+    bdir = os.path.join(CSRC, "_build")
+    os.makedirs(bdir, exist_ok=True)
+    common = [NVCC, *ARCH, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-I", os.path.join(ROOT, "include")]
+    procs, objs = [], []
+    for u in units:
+        obj = os.path.join(bdir, u.rsplit(".", 1)[0] + ".o")
+        objs.append(obj)
+        cmd = [*common, "-c", os.path.join(CSRC, u), "-o", obj]
+        print(" ".join(cmd), flush=True)
+        procs.append(subprocess.Popen(cmd))
+    if any(p.wait() != 0 for p in procs):
+        raise subprocess.CalledProcessError(1, "nvcc")
+    _run([NVCC, *ARCH, "-shared", "-o", out, *objs, "-ldl", "-lpthread"])
     return out
 
 

@@ -45,6 +45,27 @@ struct FftPlan {
     const float2* bhat;   // [m]  FFT_m(conj chirp, wrapped) / m
 };
 
+// for (i = threadIdx.x; i < n; i += blockDim.x) st(i, ld(i)), U iterations at
+// a time with their loads issued before their stores, so a thread waits for
+// global memory once per U elements rather than once per element.
+template <int U, class Ld, class St>
+__device__ __forceinline__ void staged_copy(int n, Ld ld, St st)
+{
+    for (int i0 = threadIdx.x; i0 < n; i0 += U * blockDim.x) {
+        decltype(ld(0)) v[U];
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            const int i = i0 + u * blockDim.x;
+            if (i < n) v[u] = ld(i);
+        }
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            const int i = i0 + u * blockDim.x;
+            if (i < n) st(i, v[u]);
+        }
+    }
+}
+
 __device__ __forceinline__ float2 cmul(float2 a, float2 b)
 {
     return make_float2(__fmaf_rn(a.x, b.x, -a.y * b.y), __fmaf_rn(a.x, b.y, a.y * b.x));

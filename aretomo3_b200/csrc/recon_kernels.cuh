@@ -153,27 +153,6 @@ __device__ __forceinline__ float comp(const float4& v, int q)
     return q == 0 ? v.x : q == 1 ? v.y : q == 2 ? v.z : v.w;
 }
 
-// for (i = threadIdx.x; i < n; i += blockDim.x) st(i, ld(i)), U iterations at
-// a time with their loads issued before their stores, so a thread waits for
-// global memory once per U elements rather than once per element.
-template <int U, class Ld, class St>
-__device__ __forceinline__ void staged_copy(int n, Ld ld, St st)
-{
-    for (int i0 = threadIdx.x; i0 < n; i0 += U * blockDim.x) {
-        decltype(ld(0)) v[U];
-#pragma unroll
-        for (int u = 0; u < U; u++) {
-            const int i = i0 + u * blockDim.x;
-            if (i < n) v[u] = ld(i);
-        }
-#pragma unroll
-        for (int u = 0; u < U; u++) {
-            const int i = i0 + u * blockDim.x;
-            if (i < n) st(i, v[u]);
-        }
-    }
-}
-
 // Largest magnitude over a CTA's values (non-empty ones only); every thread
 // gets the result.  Uses red[32] of shared memory.
 __device__ __forceinline__ float block_absmax(float v, float* red)

@@ -14,6 +14,7 @@ All computation runs in libat3r.so on the GPU; there is no CPU path.
 from __future__ import annotations
 
 import ctypes
+import time
 from dataclasses import dataclass, field
 
 import numpy as np
@@ -45,6 +46,21 @@ class Geom(ctypes.Structure):
         ("slab_slices", ctypes.c_int),
         ("compute_rfactor", ctypes.c_int),
     ]
+
+
+class StackGeom(ctypes.Structure):
+    """at3r_stack_geom (include/at3r.h)."""
+    _fields_ = [("nx", ctypes.c_int), ("ny", ctypes.c_int), ("n_tilts", ctypes.c_int), ("correct", ctypes.c_int),
+                ("shifts", ctypes.c_void_p), ("tilt_axes_deg", ctypes.c_void_p), ("size_axis_deg", ctypes.c_float),
+                ("num_patches", ctypes.c_int), ("local_params", ctypes.c_void_p), ("rand_fill", ctypes.c_int),
+                ("seed", ctypes.c_ulonglong), ("bin", ctypes.c_float)]
+
+
+class ThicknessResult(ctypes.Structure):
+    """at3r_thickness (include/at3r.h)."""
+    _fields_ = [("binning", ctypes.c_float), ("binned_xy", ctypes.c_int * 2), ("vol_z", ctypes.c_int),
+                ("n_profile", ctypes.c_int), ("edges", ctypes.c_int * 2), ("thickness", ctypes.c_int),
+                ("offset_z", ctypes.c_int)]
 
 
 _EXPORTS = {
@@ -91,6 +107,21 @@ _EXPORTS = {
     "at3r_reproj_host": (ctypes.c_int, [ctypes.POINTER(ctypes.c_void_p), ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                         ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
                                         ctypes.c_void_p, ctypes.c_void_p]),
+    "at3r_stack_geom_init": (None, [ctypes.POINTER(StackGeom)]),
+    "at3r_stack_create": (ctypes.c_int, [ctypes.POINTER(StackGeom), ctypes.POINTER(ctypes.c_void_p)]),
+    "at3r_stack_destroy": (None, [ctypes.c_void_p]),
+    "at3r_stack_sizes": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]),
+    "at3r_stack_c2r": (ctypes.c_int, [ctypes.c_void_p]),
+    "at3r_stack_fill_table": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t]),
+    "at3r_stack_run_device": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
+    "at3r_stack_run_host": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p),
+                                           ctypes.POINTER(ctypes.c_void_p), ctypes.c_void_p]),
+    "at3r_thickness_device": (ctypes.c_int, [ctypes.POINTER(StackGeom), ctypes.c_void_p, ctypes.c_float,
+                                             ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
+                                             ctypes.POINTER(ThicknessResult), ctypes.c_void_p]),
+    "at3r_thickness_host": (ctypes.c_int, [ctypes.POINTER(StackGeom), ctypes.c_void_p, ctypes.c_float,
+                                           ctypes.POINTER(ctypes.c_void_p), ctypes.c_void_p, ctypes.c_void_p,
+                                           ctypes.c_int, ctypes.POINTER(ThicknessResult), ctypes.c_void_p]),
     "at3r_status_str": (ctypes.c_char_p, [ctypes.c_int]),
     "at3r_last_error": (ctypes.c_char_p, []),
 }
@@ -347,11 +378,32 @@ class TiltSeries:
 
 @dataclass
 class AlignParam:
-    """Per-tilt angles in degrees, alpha offset folded in (MAM::CAlignParam::GetTilts)."""
+    """MAM::CAlignParam: per-tilt angles in degrees with the alpha offset
+    folded in (GetTilts), global shifts in pixels (GetShift) and tilt axes in
+    degrees (GetTiltAxis)."""
     tilts: np.ndarray = field(default_factory=lambda: np.zeros(0, np.float32))
+    shifts: np.ndarray | None = None       # [T][2]
+    tilt_axes: np.ndarray | None = None    # [T]
 
     def GetTilts(self, copy: bool = False):
         return self.tilts.copy() if copy else self.tilts
+
+    def GetShift(self, i: int):
+        return (0.0, 0.0) if self.shifts is None else tuple(float(v) for v in self.shifts[i])
+
+    def GetTiltAxis(self, i: int) -> float:
+        return 0.0 if self.tilt_axes is None else float(self.tilt_axes[i])
+
+
+@dataclass
+class LocalAlignParam:
+    """MAM::CLocalAlignParam: per tilt, five rows of num_patches values
+    (patch centre x, centre y, shift x, shift y, good flag), [T][5][P]."""
+    params: np.ndarray
+
+    @property
+    def m_iNumPatches(self) -> int:
+        return int(self.params.shape[2])
 
 
 def _host_run(plan: Plan, frames: np.ndarray) -> np.ndarray:
@@ -473,3 +525,213 @@ def reconstruct_device(proj, tilts, vol_z, method=WBP, out=None, stream=None, **
     s = stream if stream is not None else torch.cuda.current_stream(proj.device)
     plan.run_device(proj.data_ptr(), out.data_ptr(), s.cuda_stream)
     return out, plan
+
+
+# --- input stage and thickness measurement -----------------------------------
+
+def _stack_geom(nx, ny, n_tilts, correct=True, shifts=None, tilt_axes=None, size_axis=0.0, local_params=None,
+                rand_fill=True, seed=None, bin=1.0):
+    """at3r_stack_geom plus the arrays it points at (kept alive by the caller)."""
+    g = StackGeom()
+    lib().at3r_stack_geom_init(ctypes.byref(g))
+    g.nx, g.ny, g.n_tilts = int(nx), int(ny), int(n_tilts)
+    g.correct = int(bool(correct))
+    keep = []
+    if shifts is not None:
+        a = np.ascontiguousarray(shifts, np.float32).reshape(n_tilts, 2)
+        keep.append(a)
+        g.shifts = a.ctypes.data
+    if tilt_axes is not None:
+        a = np.ascontiguousarray(tilt_axes, np.float32).reshape(n_tilts)
+        keep.append(a)
+        g.tilt_axes_deg = a.ctypes.data
+    g.size_axis_deg = float(size_axis)
+    if local_params is not None:
+        a = np.ascontiguousarray(local_params, np.float32)
+        if a.ndim != 3 or a.shape[0] != n_tilts or a.shape[1] != 5:
+            raise ValueError("local_params must be [n_tilts][5][num_patches]")
+        keep.append(a)
+        g.num_patches = int(a.shape[2])
+        g.local_params = a.ctypes.data
+    g.rand_fill = int(bool(rand_fill))
+    g.seed = int(time.time()) if seed is None else int(seed)
+    g.bin = float(bin)
+    return g, keep
+
+
+class Stack:
+    """An at3r_stack: aligned (shift / rotation / local patches + random fill)
+    and Fourier-binned tilt frames.  Arguments as at3r_stack_geom; seed None
+    seeds the fill's table with the time, as the reference does."""
+
+    def __init__(self, nx, ny, n_tilts, **kw):
+        g, keep = _stack_geom(nx, ny, n_tilts, **kw)
+        h = ctypes.c_void_p()
+        _check(lib().at3r_stack_create(ctypes.byref(g), ctypes.byref(h)))
+        self._h = h
+        self.n_tilts = int(n_tilts)
+        self.raw_shape = (int(n_tilts), int(ny), int(nx))
+        a, b = (ctypes.c_int * 2)(), (ctypes.c_int * 2)()
+        _check(lib().at3r_stack_sizes(h, a, b))
+        self.aligned_xy = (a[0], a[1])
+        self.binned_xy = (b[0], b[1])
+        self.seed = int(g.seed)
+
+    @property
+    def binned_shape(self):
+        return (self.n_tilts, self.binned_xy[1], self.binned_xy[0])
+
+    def run_device(self, raw_ptr: int, out_ptr: int, stream: int = 0) -> None:
+        _check(lib().at3r_stack_run_device(self._h, ctypes.c_void_p(raw_ptr), ctypes.c_void_p(out_ptr),
+                                           ctypes.c_void_p(stream)))
+
+    def run_host(self, frames, out=None, stream: int = 0) -> np.ndarray:
+        frames = [np.ascontiguousarray(f, np.float32) for f in frames]
+        if out is None:
+            out = np.empty(self.binned_shape, np.float32)
+        P = ctypes.c_void_p * self.n_tilts
+        _check(lib().at3r_stack_run_host(self._h, P(*[f.ctypes.data for f in frames]),
+                                         P(*[out[t].ctypes.data for t in range(self.n_tilts)]),
+                                         ctypes.c_void_p(stream)))
+        return out
+
+    @property
+    def c2r(self) -> int:
+        """C2R convention of the binning (C2R_HERMITIAN or C2R_PACKED)."""
+        return int(lib().at3r_stack_c2r(self._h))
+
+    def fill_table(self) -> np.ndarray:
+        """The random table of the fill (W * ay entries, W = ax rounded down to even)."""
+        W = self.aligned_xy[0] & ~1
+        out = np.empty(W * self.aligned_xy[1], np.int32)
+        _check(lib().at3r_stack_fill_table(self._h, out.ctypes.data, out.size))
+        return out
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            lib().at3r_stack_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class CCorrTomoStack:
+    """Mirror of MAC::CCorrTomoStack (AreTomo/Correct/CCorrTomoStack.cpp:66-222)
+    set up with Fourier cropping: Set0(series) .. Set4, DoIt, GetCorrectedStack.
+    Set0 takes the tilt series whose size the reference reads from its series
+    package; DoIt takes the alignment (and local alignment, if Set1 was given
+    patches) the reference reads from its singletons.  Real-space binning
+    (Set2 with bFourierCrop = false) and the R-weighting of Set3 are not
+    part of this path."""
+
+    def Set0(self, tilt_series: "TiltSeries"):
+        self._series = tilt_series
+        self._corrected = None
+
+    def Set1(self, num_patches: int, tilt_axis: float):
+        self._patches, self._size_axis = int(num_patches), float(tilt_axis)
+
+    def Set2(self, out_bin: float, fourier_crop: bool = True, rand_fill: bool = True):
+        if not fourier_crop:
+            raise NotImplementedError("real-space binning (GBinImage2D) is not part of this path")
+        self._bin = float(out_bin)
+        self._rand_fill = True   # CCorrTomoStack::Set2 forces it with Fourier cropping
+
+    def Set3(self, shift_only: bool, corr_int: bool, rweight: bool):
+        if rweight:
+            raise NotImplementedError("the R-weighted corrected stack is not part of this path")
+        self._shift_only = bool(shift_only)
+
+    def Set4(self, for_recon: bool):
+        self._for_recon = bool(for_recon)
+
+    def DoIt(self, align_param: "AlignParam", local_param: "LocalAlignParam | None" = None, seed=None):
+        nx, ny, nt = self._series.stk_size
+        axes = None
+        if not self._shift_only:
+            axes = np.asarray([align_param.GetTiltAxis(i) for i in range(nt)], np.float32)
+        local = None
+        if self._patches > 0 and local_param is not None:
+            local = local_param.params
+        st = Stack(nx, ny, nt, shifts=np.asarray([align_param.GetShift(i) for i in range(nt)], np.float32),
+                   tilt_axes=axes, size_axis=self._size_axis, local_params=local, rand_fill=self._rand_fill,
+                   seed=seed, bin=self._bin)
+        try:
+            out = st.run_host([self._series.frames[t] for t in range(nt)])
+            self._aligned_xy, self._binned_xy = st.aligned_xy, st.binned_xy
+        finally:
+            st.close()
+        self._corrected = TiltSeries(out)
+        return self._corrected
+
+    def GetCorrectedStack(self, clean: bool = False) -> "TiltSeries":
+        out = self._corrected
+        if clean:
+            self._corrected = None
+        return out
+
+    def GetBinning(self):
+        """m_afBinning: aligned / binned size per dimension."""
+        return (np.float32(self._aligned_xy[0]) / np.float32(self._binned_xy[0]),
+                np.float32(self._aligned_xy[1]) / np.float32(self._binned_xy[1]))
+
+
+class CBinStack:
+    """Mirror of MAC::CBinStack::DoFFT (AreTomo/Correct/CBinStack.cpp:61-106)."""
+
+    @staticmethod
+    def DoFFT(tilt_series: "TiltSeries", bin: float) -> "TiltSeries":
+        nx, ny, nt = tilt_series.stk_size
+        st = Stack(nx, ny, nt, correct=False, rand_fill=False, seed=0, bin=bin)
+        try:
+            return TiltSeries(st.run_host([tilt_series.frames[t] for t in range(nt)]))
+        finally:
+            st.close()
+
+
+class CCalcVolThick:
+    """Mirror of MAR::CCalcVolThick (AreTomo/Recon/CCalcVolThick.cpp:47-110):
+    DoIt(series, alignment, pixel size) aligns and bins the series by
+    max(20 / pixel size, 20), reconstructs it by WBP, measures the standard
+    deviation of every z plane and finds the sample's edges.  The tilt axis of
+    tilt 0 sizes the aligned frame (Set1 of the reference's call)."""
+
+    def DoIt(self, tilt_series: "TiltSeries", align_param: "AlignParam", pix_size: float, seed=None):
+        nx, ny, nt = tilt_series.stk_size
+        axes = np.asarray([align_param.GetTiltAxis(i) for i in range(nt)], np.float32)
+        g, keep = _stack_geom(nx, ny, nt, shifts=np.asarray([align_param.GetShift(i) for i in range(nt)], np.float32),
+                              tilt_axes=axes, size_axis=float(axes[0]), rand_fill=True, seed=seed)
+        self.seed = int(g.seed)
+        tilts = np.ascontiguousarray(align_param.GetTilts(False)[:nt], np.float32)
+        frames = [np.ascontiguousarray(tilt_series.frames[t], np.float32) for t in range(nt)]
+        cap = 4096
+        prof, prof_s = np.zeros(cap, np.float32), np.zeros(cap, np.float32)
+        r = ThicknessResult()
+        P = ctypes.c_void_p * nt
+        _check(lib().at3r_thickness_host(ctypes.byref(g), tilts.ctypes.data, float(pix_size),
+                                         P(*[f.ctypes.data for f in frames]), prof.ctypes.data, prof_s.ctypes.data,
+                                         cap, ctypes.byref(r), None))
+        self.result = r
+        n = r.n_profile
+        self.profile, self.profile_smoothed = prof[:n].copy(), prof_s[:n].copy()
+        self.m_aiSampleEdges = (r.edges[0], r.edges[1])
+        self.m_fBinning = np.float32(r.binning)
+        # pixel size of the binned series, CCorrTomoStack::DoIt and CCalcVolThick.cpp:73
+        a = (ny, nx) if abs(np.sin(float(axes[0]) * 3.14 / 180.0)) > 0.707 else (nx, ny)
+        bin_y = np.float32(a[1]) / np.float32(r.binned_xy[1])
+        self.m_fPixSize = np.float32(np.float32(np.float32(pix_size) * bin_y) / self.m_fBinning)
+        return self
+
+    def GetThickness(self, angstrom: bool = False) -> float:
+        t = np.float32(self.m_aiSampleEdges[1] - self.m_aiSampleEdges[0])
+        return float(t * self.m_fPixSize) if angstrom else float(t)
+
+    def GetLowEdge(self, angstrom: bool = False) -> float:
+        return float(np.float32(self.m_aiSampleEdges[0]) * (self.m_fPixSize if angstrom else np.float32(1)))
+
+    def GetHighEdge(self, angstrom: bool = False) -> float:
+        return float(np.float32(self.m_aiSampleEdges[1]) * (self.m_fPixSize if angstrom else np.float32(1)))

@@ -236,6 +236,92 @@ size_t at3r_server_in_use_bytes(at3r_server* server);
 /* Waits for every submitted request, then releases the workers. */
 void at3r_server_destroy(at3r_server* server);
 
+/* ---- Input stage: the aligned, binned tilt series that Recon reads --------
+ * at3r_stack replaces AreTomo/Correct/CCorrTomoStack (Set0..Set4, DoIt,
+ * GetCorrectedStack; CCorrTomoStack.cpp:66-222) as CAreTomoMain::
+ * mSetupTsCorrection (CAreTomoMain.cpp:595-619) and CCalcVolThick::DoIt
+ * (CCalcVolThick.cpp:58-75) set it up, with Fourier cropping; with
+ * correct = 0 it is CBinStack::DoFFT (CBinStack.cpp:61-106).  Per tilt:
+ *   1. the aligned frame: pixel (X, Y) takes the raw pixel nearest to its
+ *      centred coordinates rotated by the frame's tilt axis, moved by the
+ *      weighted local patch shift and the global shift, or -1e30 outside the
+ *      raw frame (GCorrPatchShift.cu:18-104);
+ *   2. the random fill of those pixels (MaUtil/GFillEmpty2D.cu, table of
+ *      MaUtil/GGenRandoms.cu drawn once per stack from `seed`);
+ *   3. Fourier-crop binning: 2-D R2C normalised by 1/(ax ay), crop, 2-D C2R
+ *      (CFourierCropImage.cpp:41-61), or a plain copy when the binned size
+ *      equals the aligned size (CFourierCropImage::mCopy).
+ * Sizes: the aligned frame is ax x ay = nx x ny, or ny x nx when
+ * |sin(size_axis_deg)| > 0.707 (CCorrectUtil::CalcAlignedSize); the binned
+ * frame is bx x by = (int)(a / bin) rounded down to even per dimension, or
+ * the aligned size when bin == 1 (GFourierResize2D::GetBinnedImgSize).
+ * When ax is odd the reference's kernels cover ax - 1 columns and leave the
+ * last one unwritten; here it is 0.
+ * Layouts: raw frames [n_tilts][ny][nx]; binned frames [n_tilts][by][bx]. */
+typedef struct at3r_stack_geom {
+    int nx, ny, n_tilts;          /* raw frames */
+    int correct;                  /* 1: align (+ fill) before binning; 0: bin the frames as given */
+    const float* shifts;          /* [n_tilts][2] global shifts in pixels (CAlignParam::GetShift); NULL = 0 */
+    const float* tilt_axes_deg;   /* [n_tilts] frame rotation (CAlignParam::GetTiltAxis); NULL = shift only */
+    float size_axis_deg;          /* tilt axis the aligned size follows (CCorrTomoStack::Set1 fTiltAxis) */
+    int num_patches;              /* local-alignment patches (Set1 iNumPatches); 0 = none */
+    const float* local_params;    /* [n_tilts][5][num_patches]: centre x, centre y, shift x, shift y, good
+                                     (CLocalAlignParam::GetParam) */
+    int rand_fill;                /* fill empty pixels; CCorrTomoStack forces it with Fourier cropping */
+    unsigned long long seed;      /* seed of the fill's random table (the reference seeds with time(0)) */
+    float bin;                    /* Fourier-crop binning >= 1 (Set2 fOutBin, CBinStack::DoFFT fBin) */
+} at3r_stack_geom;
+typedef struct at3r_stack at3r_stack;
+
+/* correct = 1, rand_fill = 1, bin = 1, everything else 0 / NULL. */
+void at3r_stack_geom_init(at3r_stack_geom* g);
+/* Copies the alignment, draws the random table and plans the binning FFTs
+ * on the current device.  AT3R_ERR_TOO_LARGE when a frame dimension exceeds
+ * what one CTA's shared-memory FFT holds. */
+at3r_status at3r_stack_create(const at3r_stack_geom* g, at3r_stack** out);
+void at3r_stack_destroy(at3r_stack* stack);
+/* aligned_xy = {ax, ay}, binned_xy = {bx, by} (either may be NULL). */
+at3r_status at3r_stack_sizes(const at3r_stack* stack, int* aligned_xy, int* binned_xy);
+/* Copies the fill's random table (W * ay entries, W = ax rounded down to
+ * even; entry i is the pixel index pixel i's chain starts at) to host
+ * memory; n = its capacity in entries.  AT3R_ERR_INVALID_ARGUMENT when the
+ * stack has no fill. */
+at3r_status at3r_stack_fill_table(const at3r_stack* stack, int* table, size_t n);
+/* The C2R convention the binning follows (AT3R_C2R_HERMITIAN / PACKED, as
+ * cuFFT treats a 2-D C2R of the binned size; see at3r_c2r). */
+int at3r_stack_c2r(const at3r_stack* stack);
+/* raw, binned: device buffers in the layouts above. */
+at3r_status at3r_stack_run_device(at3r_stack* stack, const float* raw, float* binned, void* stream);
+/* frames: n_tilts host frames of nx*ny floats; binned_frames: n_tilts host
+ * frames of bx*by floats.  Returns when they are written. */
+at3r_status at3r_stack_run_host(at3r_stack* stack, const float* const* frames, float* const* binned_frames,
+                                void* stream);
+
+/* ---- Thickness measurement: CCalcVolThick::DoIt (CCalcVolThick.cpp:47-110)
+ * The series is aligned and binned by max(20 / pix_size, 20) (at3r_stack with
+ * g's shifts and tilt axes, random fill, no local patches), reconstructed by
+ * WBP with thickness (int)(bx * 0.8) / 2 * 2, and the standard deviation of a
+ * tile of every z plane of the flipped volume (CTiltSeries::FlipVol(true)) is
+ * smoothed and searched for the sample's edges (mMeasureStd, mSmooth,
+ * mDetectEdges).  tilts_deg: the tilt angles (CAlignParam::GetTilts(false)).
+ * profile / profile_smoothed (may be NULL): the vol_z - 1 plane values before
+ * and after smoothing, at most profile_cap of them. */
+typedef struct at3r_thickness {
+    float binning;        /* m_fBinning */
+    int binned_xy[2];     /* binned frame size */
+    int vol_z;            /* thickness of the low-resolution volume */
+    int n_profile;        /* vol_z - 1 */
+    int edges[2];         /* sample edges in raw pixels (m_aiSampleEdges); GetLowEdge / GetHighEdge */
+    int thickness;        /* edges[1] - edges[0]: CAlignParam::m_iThickness, GetThickness */
+    int offset_z;         /* sample centre - volume centre: CAlignParam::m_iOffsetZ */
+} at3r_thickness;
+at3r_status at3r_thickness_device(const at3r_stack_geom* g, const float* tilts_deg, float pix_size, const float* raw,
+                                  float* profile, float* profile_smoothed, int profile_cap, at3r_thickness* result,
+                                  void* stream);
+at3r_status at3r_thickness_host(const at3r_stack_geom* g, const float* tilts_deg, float pix_size,
+                                const float* const* frames, float* profile, float* profile_smoothed,
+                                int profile_cap, at3r_thickness* result, void* stream);
+
 const char* at3r_status_str(at3r_status s);
 const char* at3r_last_error(void);
 

@@ -587,6 +587,182 @@ void reproj_row(const float* const* rows, const float* tilts, const int* range, 
         out[u] = pcnt[0] < 0.8f * L ? -1e30f : part[0] / pcnt[0];
     }
 }
+
+// ---------------------------------------------------------------------------
+// Input stage (AreTomo/Correct): aligned frame, random fill, Fourier binning.
+// ---------------------------------------------------------------------------
+
+// CCorrectUtil::CalcAlignedSize (AreTomo/Correct/CCorrectUtil.cpp:11-21).
+void stack_aligned_size(int nx, int ny, float axis_deg, int* a)
+{
+    a[0] = nx;
+    a[1] = ny;
+    const double rot = std::fabs(std::sin(axis_deg * 3.14 / 180.0));
+    if (rot <= 0.707) return;
+    a[0] = ny;
+    a[1] = nx;
+}
+
+// GFourierResize2D::GetBinnedImgSize (MaUtil/GFourierResize2D.cu:75-88).
+void stack_binned_size(const int* a, float bin, int* b)
+{
+    b[0] = a[0];
+    b[1] = a[1];
+    if (bin == 1.0f) return;
+    b[0] = (int)(a[0] / bin) / 2 * 2;
+    b[1] = (int)(a[1] / bin) / 2 * 2;
+}
+
+// GCorrPatchShift.cu:61-104 (mGCorrect) and :18-49 (mGCalcLocalShift), in
+// FP32 with the fused multiply-adds the reference's compiler forms:
+// a*b - c*d -> fma(a, b, -(c*d)), a*b + c*d -> fma(a, b, c*d), s += a*b ->
+// fma(a, b, s).  W: the width the reference's grid covers; columns >= W are 0.
+void stack_corr_frame(const float* raw, int nx, int ny, int ax, int ay, int W, float shx, float shy, float c,
+                      float s, const float* local, int P, float* out)
+{
+    for (int Y = 0; Y < ay; Y++) {
+        for (int X = 0; X < ax; X++) {
+            float* o = out + (size_t)Y * ax + X;
+            if (X >= W) {
+                *o = 0.f;
+                continue;
+            }
+            float fx = ((float)X + 0.5f) - (float)W * 0.5f;
+            float fy = ((float)Y + 0.5f) - (float)ay * 0.5f;
+            const float ft = std::fmaf(fx, c, -(fy * s));
+            fy = std::fmaf(fx, s, fy * c);
+            fx = ft;
+            if (P > 0 && local) {
+                int cnt = 0;
+                float sx = 0.f, sy = 0.f, sw = 0.f;
+                for (int p = 0; p < P; p++) {
+                    if (local[4 * P + p] < 0.9f) continue;
+                    const float lx = (fx - local[p]) / (float)nx;
+                    const float ly = (fy - local[P + p]) / (float)ny;
+                    const float w = std::exp(-100.0f * std::fmaf(lx, lx, ly * ly));
+                    sx = std::fmaf(local[2 * P + p], w, sx);
+                    sy = std::fmaf(local[3 * P + p], w, sy);
+                    sw += w;
+                    cnt++;
+                }
+                float dx = 0.f, dy = 0.f;
+                if (cnt > 0) {
+                    dx = sx / sw;
+                    dy = sy / sw;
+                }
+                fx += dx;
+                fy += dy;
+            }
+            fx += (shx + (float)nx * 0.5f);
+            fy += (shy + (float)ny * 0.5f);
+            const int x = (int)(fx + 0.5f), y = (int)(fy + 0.5f);
+            *o = (x >= 0 && x < nx && y >= 0 && y < ny) ? raw[(size_t)y * nx + x] : kSentinelValue;
+        }
+    }
+}
+
+// GFillEmpty2D.cu:7-87: empty = value < -1e10; the mean of the non-empty
+// pixels as one 512-thread block sums it (strided float partial sums, then a
+// halving tree); every empty pixel follows its random chain (at most 100
+// links) to the first non-empty pixel, else takes the mean.
+void stack_fill_frame(float* img, int W, int ax, int ay, const int* table)
+{
+    const int n = W * ay;
+    std::vector<unsigned char> empty(n);
+    for (int i = 0; i < n; i++) empty[i] = img[(size_t)(i / W) * ax + i % W] < kSentinelTest;
+    float psum[512], pcnt[512];
+    for (int t = 0; t < 512; t++) {
+        float sum = 0.f, cnt = 0.f;
+        for (int i = t; i < n; i += 512) {
+            if (empty[i]) continue;
+            sum += img[(size_t)(i / W) * ax + i % W];
+            cnt += 1.0f;
+        }
+        psum[t] = sum;
+        pcnt[t] = cnt;
+    }
+    for (int off = 256; off > 0; off /= 2)
+        for (int t = 0; t < off; t++) {
+            psum[t] += psum[t + off];
+            pcnt[t] += pcnt[t + off];
+        }
+    const float mean = pcnt[0] <= 0.f ? 0.f : psum[0] / pcnt[0];
+    std::vector<float> src(img, img + (size_t)ay * ax);
+    for (int i = 0; i < n; i++) {
+        if (!empty[i]) continue;
+        float v = mean;
+        int next = table[i];
+        for (int j = 0; j < 100; j++) {
+            if (empty[next]) {
+                next = table[next];
+                continue;
+            }
+            v = src[(size_t)(next / W) * ax + next % W];
+            break;
+        }
+        img[(size_t)(i / W) * ax + i % W] = v;
+    }
+}
+
+// Fourier-crop binning (CFourierCropImage.cpp:41-61 = CBinStack::DoFFT per
+// frame): 2-D R2C of (ay x ax) scaled by 1/(ax ay) (MaUtil/CCufft2D.cpp:65-86),
+// crop to (by x bx) as GFourierResize2D.cu:7-39 does, 2-D C2R unnormalised
+// under the selected C2R convention.  A binned size equal to the aligned size
+// is a copy (CFourierCropImage::mCopy).
+template <class R>
+void stack_bin_frame(const float* img, int ax, int ay, int bx, int by, R* out)
+{
+    if (ax == bx && ay == by) {
+        for (size_t i = 0; i < (size_t)ax * ay; i++) out[i] = img[i];
+        return;
+    }
+    const int KX = bx / 2 + 1;
+    std::vector<std::complex<R>> rows((size_t)ay * KX), line(ax);
+    for (int y = 0; y < ay; y++) {
+        for (int x = 0; x < ax; x++) line[x] = std::complex<R>((R)img[(size_t)y * ax + x], 0);
+        fft<R>(line.data(), ax, -1);
+        for (int k = 0; k < KX; k++) rows[(size_t)y * KX + k] = line[k];
+    }
+    const R norm = (R)(1.0 / ax / ay);
+    std::vector<std::complex<R>> crop((size_t)by * KX), col(ay), col2(by);
+    for (int k = 0; k < KX; k++) {
+        for (int y = 0; y < ay; y++) col[y] = rows[(size_t)y * KX + k];
+        fft<R>(col.data(), ay, -1);
+        for (int ky = 0; ky < by; ky++) {
+            const int src = ky <= by / 2 ? ky : ky + ay - by;
+            col2[ky] = col[src] * norm;
+        }
+        fft<R>(col2.data(), by, +1);
+        for (int y = 0; y < by; y++) crop[(size_t)y * KX + k] = col2[y];
+    }
+    for (int y = 0; y < by; y++) c2r<R>(&crop[(size_t)y * KX], bx, out + (size_t)y * bx, g_c2r_mode);
+}
+
+// CCalcVolThick::mMeasureStd (CCalcVolThick.cpp:172-197) on plane k of
+// FlipVol(true) of vol[ny][Nz][Nx]: rows j in [0, ty) (from row 0, as the
+// reference indexes them), columns x0 .. x0 + tx - 1; sums in double in the
+// reference's order.
+float thick_plane_std(const float* vol, int Nx, int Nz, int k, int x0, int tx, int ty)
+{
+    const int zr = Nz - 1 - k;
+    double s1 = 0.0, s2 = 0.0;
+    int cnt = 0;
+    for (int j = 0; j < ty; j++) {
+        const float* row = vol + ((size_t)j * Nz + zr) * Nx + x0;
+        for (int i = 0; i < tx; i++) {
+            const float v = row[i];
+            if (v < (float)-1e20) continue;
+            s1 += v;
+            s2 += (v * v);
+            cnt += 1;
+        }
+    }
+    s1 = s1 / cnt;
+    s2 = s2 / cnt - s1 * s1;
+    if (s2 <= 0) s2 = 0.0f;
+    else s2 = sqrtf((float)s2);
+    return (float)s2;
+}
 }  // namespace
 
 extern "C" {
@@ -695,6 +871,112 @@ int oracle_reproj_f32(const float* frames, int nx, int ny, int n_tilts, const fl
                        out + (size_t)y * nx);
         }
     }
+    return 0;
+}
+
+/* ---- input stage and thickness ------------------------------------------ */
+
+int oracle_stack_sizes(int nx, int ny, int correct, float size_axis_deg, float bin, int* sizes)
+{
+    if (!sizes || nx < 2 || ny < 2) return -1;
+    int a[2] = {nx, ny}, b[2];
+    if (correct) stack_aligned_size(nx, ny, size_axis_deg, a);
+    stack_binned_size(a, bin, b);
+    sizes[0] = a[0];
+    sizes[1] = a[1];
+    sizes[2] = b[0];
+    sizes[3] = b[1];
+    return 0;
+}
+
+int oracle_stack_f64(const float* raw, int nx, int ny, int n_tilts, int correct, const float* shifts,
+                     const float* axes_deg, float size_axis_deg, int num_patches, const float* local,
+                     int rand_fill, const int* table, float bin, double* out, float* aligned, int n_threads)
+{
+    int sz[4];
+    if (!raw || !out || oracle_stack_sizes(nx, ny, correct, size_axis_deg, bin, sz)) return -1;
+    if (correct && rand_fill && !table) return -2;
+    const int ax = sz[0], ay = sz[1], bx = sz[2], by = sz[3];
+    const int W = ((ax / 2 + 1) * 2 / 2 - 1) * 2;
+    const float d2r = 3.141592654f / 180.0f;
+    const int nth = n_threads > 0 ? n_threads : 1;
+#pragma omp parallel for num_threads(nth) schedule(dynamic, 1)
+    for (int t = 0; t < n_tilts; t++) {
+        std::vector<float> img((size_t)ax * ay);
+        const float* src = raw + (size_t)t * nx * ny;
+        if (correct) {
+            const float rad = axes_deg ? axes_deg[t] * d2r : 0.f;
+            const float c = std::cos(rad), s = std::sin(rad);
+            stack_corr_frame(src, nx, ny, ax, ay, W, shifts ? shifts[2 * t] : 0.f, shifts ? shifts[2 * t + 1] : 0.f,
+                             c, s, local ? local + (size_t)t * 5 * num_patches : nullptr, num_patches, img.data());
+            if (rand_fill) stack_fill_frame(img.data(), W, ax, ay, table);
+        } else {
+            std::memcpy(img.data(), src, sizeof(float) * img.size());
+        }
+        if (aligned) std::memcpy(aligned + (size_t)t * ax * ay, img.data(), sizeof(float) * img.size());
+        stack_bin_frame<double>(img.data(), ax, ay, bx, by, out + (size_t)t * bx * by);
+    }
+    return 0;
+}
+
+int oracle_stack_fill_f32(float* img, int W, int ax, int ay, const int* table)
+{
+    if (!img || !table || W < 1 || W > ax || ay < 1) return -1;
+    stack_fill_frame(img, W, ax, ay, table);
+    return 0;
+}
+
+int oracle_thickness_profile(const float* vol, int Nx, int ny, int vol_z, float* profile)
+{
+    if (!vol || !profile || Nx < 2 || ny < 1 || vol_z < 2) return -1;
+    const int tx = (int)(Nx * 0.4f) / 2 * 2, ty = (int)(ny * 0.4f) / 2 * 2;
+    const int x0 = (Nx - tx) / 2;
+    for (int k = 0; k < vol_z - 1; k++) profile[k] = thick_plane_std(vol, Nx, vol_z, k, x0, tx, ty);
+    return 0;
+}
+
+int oracle_thickness_edges(const float* profile, int n, float bin, float* smoothed, int* result)
+{
+    if (!profile || !result || n < 10) return -1;
+    // CCalcVolThick::mSmooth (CCalcVolThick.cpp:114-132)
+    std::vector<float> cc(n);
+    for (int i = 0; i < n; i++) {
+        const int start = i - 5;
+        double sum = 0.0;
+        for (int j = 0; j < 11; j++) {
+            const int k = std::min(std::max(j + start, 0), n - 1);
+            sum += profile[k];
+        }
+        cc[i] = (float)sum / 11;
+    }
+    if (smoothed) std::memcpy(smoothed, cc.data(), sizeof(float) * n);
+    // CCalcVolThick::mDetectEdges (CCalcVolThick.cpp:209-284); an edge that
+    // no sample reaches stays at its search bound
+    const int half = n / 2, bot = (int)(n * 0.1), top = n - bot;
+    float mean = 0.f;
+    for (int i = bot; i < top; i++) mean += cc[i];
+    mean = mean / (top - bot);
+    int e0 = bot, e1 = top;
+    for (int i = bot; i < half; i++)
+        if (cc[i] >= mean) { e0 = i; break; }
+    float minv = mean;
+    int imin = e0;
+    for (int i = bot; i < e0; i++)
+        if (cc[i] < minv) { minv = cc[i]; imin = i; }
+    e0 = (e0 + imin) / 2;
+    for (int i = top; i > half; i--)
+        if (cc[i] >= mean) { e1 = i; break; }
+    minv = mean;
+    imin = e1;
+    for (int i = top; i > e1; i--)
+        if (cc[i] < minv) { minv = cc[i]; imin = i; }
+    e1 = (e1 + imin) / 2;
+    e0 = (int)(e0 * bin);
+    e1 = (int)(e1 * bin);
+    result[0] = e0;
+    result[1] = e1;
+    result[2] = e1 - e0;
+    result[3] = (e0 + e1) / 2 - (int)(half * bin);
     return 0;
 }
 

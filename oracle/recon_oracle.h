@@ -62,6 +62,29 @@ int oracle_reproj_range(const float* tilts_deg, const unsigned char* skip, int n
 int oracle_reproj_f32(const float* frames, int nx, int ny, int n_tilts, const float* tilts_deg,
                       const unsigned char* skip, int proj_idx, int vol_z, float* out, int n_threads);
 
+/* Input stage (AreTomo/Correct/CCorrTomoStack.cpp with Fourier cropping;
+ * correct = 0: CBinStack::DoFFT).  sizes = {ax, ay, bx, by}: the aligned
+ * (CCorrectUtil::CalcAlignedSize) and binned (GFourierResize2D::
+ * GetBinnedImgSize) frame sizes. */
+int oracle_stack_sizes(int nx, int ny, int correct, float size_axis_deg, float bin, int* sizes);
+/* raw [T][ny][nx] -> out [T][by][bx] in FP64 after the FP32 aligned frame
+ * (GCorrPatchShift.cu) and the random fill (GFillEmpty2D.cu) driven by
+ * `table` (W * ay entries, W = the width the reference's kernels cover; as
+ * GGenRandoms draws it).  shifts [T][2], axes_deg [T] (NULL = 0), local
+ * [T][5][num_patches] (may be NULL).  aligned (may be NULL): the filled
+ * aligned frames [T][ay][ax]. */
+int oracle_stack_f64(const float* raw, int nx, int ny, int n_tilts, int correct, const float* shifts,
+                     const float* axes_deg, float size_axis_deg, int num_patches, const float* local,
+                     int rand_fill, const int* table, float bin, double* out, float* aligned, int n_threads);
+/* The fill alone on one frame img[ay][ax] (columns [0, W) covered). */
+int oracle_stack_fill_f32(float* img, int W, int ax, int ay, const int* table);
+/* Thickness measurement (AreTomo/Recon/CCalcVolThick.cpp): plane standard
+ * deviations of FlipVol(true) of vol[ny][vol_z][Nx] (vol_z - 1 values,
+ * mMeasureStd), then smoothing and edge detection (mSmooth, mDetectEdges):
+ * result = {low edge, high edge, thickness, z offset} in raw pixels. */
+int oracle_thickness_profile(const float* vol, int Nx, int ny, int vol_z, float* profile);
+int oracle_thickness_edges(const float* profile, int n, float bin, float* smoothed, int* result);
+
 /* Components, for known-answer tests. */
 /* complex FFT of length n, interleaved re/im; sign -1 forward, +1 inverse, unnormalised */
 int oracle_fft_f64(const double* in, int n, int sign, double* out);

@@ -4,7 +4,9 @@
 # sm_100a from the reference sources where they lie, plus this directory's
 # driver and stub, into oracle/_ref/ref_recon; and its projection-alignment
 # re-projector (AreTomo/ProjAlign/GReproj + CCalcReproj) into
-# oracle/_ref/ref_reproj.  Nothing is copied out of the
+# oracle/_ref/ref_reproj; and its input stage (AreTomo/Correct/GCorrPatchShift
+# + the Fourier crop of CFourierCropImage) with the thickness measurement
+# (AreTomo/Recon/CCalcVolThick) into oracle/_ref/ref_stack.  Nothing is copied out of the
 # reference tree; objects go to oracle/_ref/obj.
 set -euo pipefail
 REF=${AT3R_REFERENCE:-/root/reference}
@@ -55,3 +57,22 @@ done
 g++ $CXXFLAGS -c "$HERE/ref_reproj_driver.cpp" -o "$OBJ/ref_reproj_driver.o"
 $NVCC -gencode arch=compute_100a,code=sm_100a -o "$OUT/ref_reproj" "${rp[@]}" "$OBJ/ref_reproj_driver.o"
 echo "built $OUT/ref_reproj"
+
+# the input stage (AreTomo/Correct/GCorrPatchShift.cu, CCorrectUtil.cpp) and the
+# thickness measurement (AreTomo/Recon/CCalcVolThick.cpp) on top of the Recon objects
+st=()
+for f in AreTomo/Correct/GCorrPatchShift; do
+  o="$OBJ/$(echo "$f" | tr / _).o"
+  [ "$o" -nt "$REF/$f.cu" ] || $NVCC $CUFLAGS -c "$REF/$f.cu" -o "$o"
+  st+=("$o")
+done
+for f in AreTomo/Correct/CCorrectUtil AreTomo/Recon/CCalcVolThick; do
+  o="$OBJ/$(echo "$f" | tr / _).o"
+  [ "$o" -nt "$REF/$f.cpp" ] || g++ $CXXFLAGS -c "$REF/$f.cpp" -o "$o"
+  st+=("$o")
+done
+g++ $CXXFLAGS -c "$HERE/ref_stack_stub.cpp" -o "$OBJ/ref_stack_stub.o"
+g++ $CXXFLAGS -c "$HERE/ref_stack_driver.cpp" -o "$OBJ/ref_stack_driver.o"
+$NVCC -gencode arch=compute_100a,code=sm_100a -o "$OUT/ref_stack" "${objs[@]}" "${st[@]}" \
+  "$OBJ/ref_stub.o" "$OBJ/ref_stack_stub.o" "$OBJ/ref_stack_driver.o" -lcufft -lcurand -lcuda
+echo "built $OUT/ref_stack"

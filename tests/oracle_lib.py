@@ -98,3 +98,93 @@ def reproj(frames, tilts, proj_idx, vol_z, skip=None, threads=os.cpu_count()):
     if rc != 0:
         raise ValueError(f"oracle reproj rc={rc}")
     return out
+
+
+# --- input stage and thickness ------------------------------------------------
+
+def stack_sizes(nx, ny, correct=True, size_axis=0.0, bin=1.0):
+    s = np.zeros(4, np.int32)
+    if lib().oracle_stack_sizes(int(nx), int(ny), int(bool(correct)), ctypes.c_float(size_axis),
+                                ctypes.c_float(bin), _p(s)) != 0:
+        raise ValueError("oracle stack sizes")
+    return (int(s[0]), int(s[1])), (int(s[2]), int(s[3]))
+
+
+def stack(raw, correct=True, shifts=None, tilt_axes=None, size_axis=0.0, local_params=None, rand_fill=True,
+          table=None, bin=1.0, c2r_mode=0, threads=os.cpu_count()):
+    """FP64 restatement of the input stage; returns (binned [T][by][bx] f64,
+    aligned-and-filled [T][ay][ax] f32)."""
+    raw = np.ascontiguousarray(raw, np.float32)
+    T, ny, nx = raw.shape
+    (ax, ay), (bx, by) = stack_sizes(nx, ny, correct, size_axis, bin)
+    out = np.zeros((T, by, bx), np.float64)
+    aligned = np.zeros((T, ay, ax), np.float32)
+    keep = []
+
+    def arr(a, dt):
+        if a is None:
+            return None
+        a = np.ascontiguousarray(a, dt)
+        keep.append(a)
+        return _p(a)
+    P = 0 if local_params is None else int(np.asarray(local_params).shape[2])
+    L = lib()
+    L.oracle_set_c2r_mode(int(c2r_mode))
+    rc = L.oracle_stack_f64(_p(raw), nx, ny, T, int(bool(correct)), arr(shifts, np.float32),
+                            arr(tilt_axes, np.float32), ctypes.c_float(size_axis), P, arr(local_params, np.float32),
+                            int(bool(rand_fill)), arr(table, np.int32), ctypes.c_float(bin), _p(out), _p(aligned),
+                            int(threads))
+    if rc != 0:
+        raise ValueError(f"oracle stack rc={rc}")
+    return out, aligned
+
+
+def stack_fill(img, W, table):
+    img = np.ascontiguousarray(img, np.float32).copy()
+    ay, ax = img.shape
+    t = np.ascontiguousarray(table, np.int32)
+    if lib().oracle_stack_fill_f32(_p(img), int(W), ax, ay, _p(t)) != 0:
+        raise ValueError("oracle fill")
+    return img
+
+
+def thickness_profile(vol):
+    """vol [ny][vol_z][Nx] float32 -> plane standard deviations (vol_z - 1)."""
+    vol = np.ascontiguousarray(vol, np.float32)
+    ny, nz, nx = vol.shape
+    out = np.zeros(nz - 1, np.float32)
+    if lib().oracle_thickness_profile(_p(vol), nx, ny, nz, _p(out)) != 0:
+        raise ValueError("oracle thickness profile")
+    return out
+
+
+def thickness_edges(profile, bin):
+    """-> (smoothed profile, (low edge, high edge, thickness, z offset))."""
+    p = np.ascontiguousarray(profile, np.float32)
+    sm = np.zeros_like(p)
+    r = np.zeros(4, np.int32)
+    if lib().oracle_thickness_edges(_p(p), p.size, ctypes.c_float(bin), _p(sm), _p(r)) != 0:
+        raise ValueError("oracle thickness edges")
+    return sm, tuple(int(v) for v in r)
+
+
+def load_npz(name):
+    """A fixture's arrays and its decoded meta."""
+    import json
+    z = np.load(os.path.join(ROOT, "tests", "golden", name + ".npz"))
+    d = {k: z[k] for k in z.files if k != "meta"}
+    return d, json.loads(str(z["meta"]))
+
+
+def golden_exists(name):
+    return os.path.exists(os.path.join(ROOT, "tests", "golden", name + ".npz"))
+
+
+def flip_vol(vol_xzy):
+    """CTiltSeries::FlipVol(true): XZ frames [ny][Nz][Nx] -> XY frames [Nz][ny][Nx], z reversed."""
+    return np.ascontiguousarray(np.asarray(vol_xzy).transpose(1, 0, 2)[::-1])
+
+
+def unflip_vol(vol_xyz):
+    """Inverse of flip_vol."""
+    return np.ascontiguousarray(np.asarray(vol_xyz)[::-1].transpose(1, 0, 2))

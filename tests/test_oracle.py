@@ -13,7 +13,7 @@ from oracle_lib import P, lib, load_golden, rel_l2, sart, wbp
 
 GOLDEN = sorted(n for n in (os.path.basename(f)[:-4] for f in glob.glob(os.path.join(os.path.dirname(__file__),
                                                                                   "golden", "*.npz")))
-                if not n.startswith("reproj_"))
+                if not n.startswith(("reproj_", "stack_", "thick_")))
 
 # FP64 oracle vs the reference's FP32 CUDA result: the reference accumulates in
 # FP32 (and SART iterates 15 times), so the two agree to ~1e-6 relative L2.
