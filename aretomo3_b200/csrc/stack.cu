@@ -141,7 +141,7 @@ at3r_status run_chunk(at3r_stack* s, const float* raw, int t0, int n, float* out
     const float* src = raw;
     if (s->g.correct) {
         const int fill = s->g.rand_fill ? 1 : 0;
-        k_corr<<<dim3((s->ax + 255) / 256, s->ay, n), 256, 0, st>>>(
+        k_corr<<<dim3((s->ax + 31) / 32, (s->ay + 7) / 8, n), 256, 0, st>>>(
             raw, s->nx, s->ny, s->ax, s->ay, s->W, s->d_shift + t0, s->d_cs + t0,
             s->d_local ? s->d_local + (size_t)t0 * 5 * s->P : nullptr, s->P, fill, s->d_aln, s->d_empty);
         ST_CUDA(cudaGetLastError());
@@ -375,7 +375,7 @@ at3r_status at3r_stack_create(const at3r_stack_geom* g, at3r_stack** out)
         s->smem_row = 2 * sizeof(float2) * fft_pitch(s->frow.plan.work) * s->b_row;
         s->smem_c2r = 2 * sizeof(float2) * fft_pitch(s->fbx.plan.work) * s->b_c2r;
         s->col_pitch = (fft_pitch(std::max(s->fcin.plan.work, s->fcout.plan.work)) + 1) / 2 * 2 + 1;
-        s->cb = std::max(4, std::min(32, 4096 / s->ay));
+        s->cb = std::max(1, std::min(32, 4096 / s->ay));
         while (s->cb > 1 && 2 * sizeof(float2) * s->cb * s->col_pitch > 227 * 1024) s->cb /= 2;
         s->smem_col = 2 * sizeof(float2) * s->cb * s->col_pitch;
         s->rs_col = std::max(s->fcin.rs, s->fcout.rs);

@@ -53,14 +53,20 @@ __global__ void k_axis_cs(const float* __restrict__ rad, int T, float2* __restri
 // the raw frame.  Columns X >= W (the odd-width case) are 0.  With `fill`,
 // the empty mask of the fill is written alongside.
 // local: [T][5][P] = patch centre x, centre y, shift x, shift y, good flag.
-// Grid (ceil(ax / 256), ay, T), 256 threads.
+// A CTA covers a 32 x 8 tile, each warp an 8 x 4 patch of it, so that the
+// raw pixels a warp gathers lie within a few rows and columns whatever the
+// rotation (a 32 x 1 warp on a frame rotated by ~90 degrees would read 32 raw
+// rows).  Grid (ceil(ax / 32), ceil(ay / 8), T), 256 threads.
 __global__ void __launch_bounds__(256) k_corr(const float* __restrict__ raw, int nx, int ny, int ax, int ay, int W,
                                               const float2* __restrict__ shifts, const float2* __restrict__ cs,
                                               const float* __restrict__ local, int P, int fill,
                                               float* __restrict__ aln, uint8_t* __restrict__ empty)
 {
-    const int X = blockIdx.x * blockDim.x + threadIdx.x, Y = blockIdx.y, t = blockIdx.z;
-    if (X >= ax) return;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int X = blockIdx.x * 32 + (warp & 3) * 8 + (lane & 7);
+    const int Y = blockIdx.y * 8 + (warp >> 2) * 4 + (lane >> 3);
+    const int t = blockIdx.z;
+    if (X >= ax || Y >= ay) return;
     float* o = aln + ((size_t)t * ay + Y) * ax;
     if (X >= W) {
         o[X] = 0.f;

@@ -701,6 +701,223 @@ def run_serving_arm(args):
     print(json.dumps(line), flush=True)
 
 
+# --- input stage (aligned + Fourier-binned series) and thickness ------------
+STACK_METRIC = "GPixel·tilt/s of raw frames aligned and Fourier-binned (input stage)"
+STACK_UNIT = "GPixel·tilt/s"
+
+
+def stack_workload(name: str, seed: int = 3) -> dict:
+    """The 4096 x 4096 x 41 series of the precision workload, aligned as a
+    K3-style series: per-tilt shifts of +-20 px, tilt axis 85-87 degrees (x / y
+    swapped), seeded random fill; binned by 4 (stack_4k) or measured for
+    thickness at binning 20 (thick_4k, pixel size 1)."""
+    from aretomo3_b200 import synth
+    c = synth.precision_4k(seed=seed)
+    rng = np.random.default_rng(seed)
+    T = len(c["tilts"])
+    c.update(name=name, shifts=rng.uniform(-20, 20, (T, 2)).astype(np.float32),
+             axes=rng.uniform(85.0, 87.0, T).astype(np.float32), seed=4242, bin=4.0, pix=1.0)
+    if name == "stack_4k":
+        c["label"] = ("input stage 4096x4096x41 tilts: shift +-20 px, tilt axis 85-87 deg (x/y swap), random fill, "
+                      "Fourier-crop binning 4 -> 1024x1024")
+    else:
+        c["label"] = ("thickness measurement 4096x4096x41 tilts, pixel size 1: align + bin 20, WBP 204x204, "
+                      "plane statistics, edges")
+    return c
+
+
+def stack_bytes_per_tilt(ax, ay, nx, ny, bx, by) -> float:
+    """Compulsory DRAM bytes per tilt of the stack's kernels: raw read and
+    aligned + mask write (k_corr), mask read (k_fill), aligned read and row
+    spectra write (k_bin_r2c), spectra read / cropped write (k_bin_cols),
+    cropped read and binned write (k_bin_c2r)."""
+    W = ax & ~1
+    kx = bx // 2 + 1
+    return (4.0 * nx * ny + 4.0 * ax * ay + W * ay) + W * ay + (4.0 * ax * ay + 8.0 * kx * ay) + \
+        (8.0 * kx * ay + 8.0 * kx * by) + (8.0 * kx * by + 4.0 * bx * by)
+
+
+def run_stack_arm(args):
+    import torch
+    from aretomo3_b200 import recon
+    c = stack_workload(args.workload)
+    frames = synth_frames(c)
+    if args.tilts:
+        # a smaller case of the same frames (profiling)
+        n = args.tilts
+        frames = np.ascontiguousarray(frames[:n])
+        c.update(tilts=c["tilts"][:n], shifts=c["shifts"][:n], axes=c["axes"][:n])
+        c["label"] += f"; first {n} tilts"
+    T, ny, nx = frames.shape
+    torch.cuda.set_device(0)
+    stream = torch.cuda.current_stream()
+    if args.workload == "thick_4k":
+        return run_thick_arm(args, c, frames)
+    st = recon.Stack(nx, ny, T, shifts=c["shifts"], tilt_axes=c["axes"], size_axis=float(c["axes"][0]),
+                     seed=c["seed"], bin=c["bin"])
+    (ax, ay), (bx, by) = st.aligned_xy, st.binned_xy
+    raw = torch.from_numpy(frames).cuda()
+    out = torch.empty(st.binned_shape, device="cuda", dtype=torch.float32)
+    for _ in range(args.warmup):
+        st.run_device(raw.data_ptr(), out.data_ptr(), stream.cuda_stream)
+    torch.cuda.synchronize()
+    clocks = ClockSampler(0)
+    clocks.start()
+    time.sleep(0.3)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        st.run_device(raw.data_ptr(), out.data_ptr(), stream.cuda_stream)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    ms = e0.elapsed_time(e1) / args.steps
+    units = float(nx) * ny * T
+    dev_out = out.cpu().numpy()
+    # e2e through the host entry point: pinned frames in and out
+    pin_in = torch.from_numpy(frames).pin_memory()
+    pin_out = torch.empty(st.binned_shape, dtype=torch.float32).pin_memory()
+    fin = [pin_in[t].numpy() for t in range(T)]
+    st.run_host(fin, pin_out.numpy())
+    torch.cuda.synchronize()
+    g0, g1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    g0.record(stream)
+    for _ in range(args.steps):
+        st.run_host(fin, pin_out.numpy(), stream.cuda_stream)
+    g1.record(stream)
+    torch.cuda.synchronize()
+    ms_e2e = g0.elapsed_time(g1) / args.steps
+    host_ok = bool(np.array_equal(pin_out.numpy(), dev_out))
+    # pageable frames, as CTiltSeries holds them
+    t = time.perf_counter()
+    st.run_host([f for f in frames], np.empty(st.binned_shape, np.float32))
+    ms_pageable = (time.perf_counter() - t) * 1e3
+    peaks = measured_peaks()
+    bpt = stack_bytes_per_tilt(ax, ay, nx, ny, bx, by)
+    achieved = bpt * T / (ms / 1e3) / 1e9
+    line = {
+        "metric": STACK_METRIC, "value": units / (ms / 1e3) / 1e9, "unit": STACK_UNIT, "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": c["label"], "name": c["name"], "aligned": [ax, ay], "binned": [bx, by],
+                   "l2": "inputs larger than L2 (2.75 GB of frames)"},
+        "e2e": {"value": units / (ms_e2e / 1e3) / 1e9, "unit": STACK_UNIT, "ms_per_step": ms_e2e,
+                "h2d_bytes_per_step": int(frames.nbytes), "d2h_bytes_per_step": int(4 * T * bx * by),
+                "host_equals_device": host_ok, "pageable_ms": ms_pageable},
+        "gpu_launches": int(args.steps * 6),
+        "roofline": {"bound": "hbm", "kernel": "all stack kernels (k_corr, k_fill, k_fill_mean, k_bin_r2c, "
+                                               "k_bin_cols, k_bin_c2r)",
+                     "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                     "frac": achieved / peaks["hbm_gbs"], "peak_source": peaks["source"],
+                     "traffic": None, "bytes_per_step": bpt * T},
+        "clocks": clk,
+    }
+    st.close()
+    if not args.no_cpu_baseline:
+        line["cpu_baseline"] = stack_cpu_baseline(c, frames)
+        line["reference_cuda"] = stack_reference_cuda(c, frames)
+        line["error"] = stack_error(c, frames, dev_out, (ax, ay), (bx, by))
+    print(json.dumps(line), flush=True)
+
+
+def synth_frames(c):
+    from aretomo3_b200 import synth
+    return synth.make_tilt_series(c["nx"], c["ny"], c["tilts"], c["vol_z"], c["phantom"])
+
+
+def stack_cpu_baseline(c, frames, n=None):
+    """The FP64 oracle's restatement of the stage (the reference's stage is
+    GPU-only) on a sample of tilts, one tilt per host thread."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_lib as ol
+    threads = os.cpu_count() or 1
+    n = n or min(len(c["tilts"]), threads)
+    table = np.arange((4096 & ~1) * 4096, dtype=np.int32)[::-1].copy()   # any valid chain table for timing
+    t = time.perf_counter()
+    ol.stack(frames[:n], shifts=c["shifts"][:n], tilt_axes=c["axes"][:n], size_axis=float(c["axes"][0]),
+             table=table, bin=c["bin"], threads=threads)
+    dt = time.perf_counter() - t
+    units = float(c["nx"]) * c["ny"] * n
+    return {"value": units / dt / 1e9, "unit": STACK_UNIT, "cores": threads, "kind": "port",
+            "sample": f"{n} of {len(c['tilts'])} tilts, FP64 C++ restatement, one tilt per thread, {dt:.2f} s"}
+
+
+def stack_reference_cuda(c, frames):
+    """The reference's own CUDA input stage (oracle/_ref/ref_stack, built from
+    its sources): GCorrPatchShift + the Fourier crop of CFourierCropImage per
+    tilt, with its per-tilt host copies, on the same series."""
+    exe = os.path.join(ROOT, "oracle", "_ref", "ref_stack")
+    if not os.path.exists(exe):
+        return None
+    T, ny, nx = frames.shape
+    d = "/dev/shm" if os.path.isdir("/dev/shm") else None
+    with tempfile.TemporaryDirectory(dir=d) as td:
+        fin, fpar, fout = (os.path.join(td, n) for n in ("in.bin", "par.bin", "out.bin"))
+        with open(fin, "wb") as f:
+            np.array([nx, ny, T], np.int32).tofile(f)
+            np.asarray(c["tilts"], np.float32).tofile(f)
+            frames.tofile(f)
+        with open(fpar, "wb") as f:
+            np.array([0, 0], np.int32).tofile(f)
+            c["shifts"].tofile(f)
+            c["axes"].tofile(f)
+        r = subprocess.run([exe, "stack", fin, fpar, fout, str(c["seed"]), repr(c["bin"]), repr(float(c["axes"][0])),
+                            "noaligned"], capture_output=True, text=True, timeout=600)
+        if r.returncode != 0:
+            return {"error": r.stderr[-300:]}
+        info = json.loads([ln for ln in r.stdout.splitlines() if ln.startswith("{")][-1])
+    sec = info["seconds"]
+    return {"value": float(nx) * ny * T / sec / 1e9, "unit": STACK_UNIT, "seconds": sec,
+            "what": "reference CUDA CCorrTomoStack path per tilt: pageable H2D, GCorrPatchShift + fill, "
+                    "2-D cuFFT crop, row-wise unpad to host"}
+
+
+def stack_error(c, frames, out, aligned_xy, binned_xy, n=2):
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_lib as ol
+    from aretomo3_b200 import recon
+    T = frames.shape[0]
+    st = recon.Stack(c["nx"], c["ny"], T, shifts=c["shifts"], tilt_axes=c["axes"], size_axis=float(c["axes"][0]),
+                     seed=c["seed"], bin=c["bin"])
+    try:
+        table, mode = st.fill_table(), (1 if st.c2r == recon.C2R_PACKED else 0)
+    finally:
+        st.close()
+    ref, _ = ol.stack(frames[:n], shifts=c["shifts"][:n], tilt_axes=c["axes"][:n], size_axis=float(c["axes"][0]),
+                      table=table, bin=c["bin"], c2r_mode=mode)
+    got = out[:n].astype(np.float64)
+    return {"rel_l2": float(np.linalg.norm(got - ref) / np.linalg.norm(ref)), "tilts": n,
+            "against": "FP64 oracle (host cos/sin; see tests for the bit-exact pin against the reference)"}
+
+
+def run_thick_arm(args, c, frames):
+    import torch
+    from aretomo3_b200 import recon
+    T = frames.shape[0]
+    ap = recon.AlignParam(tilts=c["tilts"], shifts=c["shifts"], tilt_axes=c["axes"])
+    pin = torch.from_numpy(frames).pin_memory()
+    ts = recon.TiltSeries(pin.numpy())
+    for _ in range(args.warmup):
+        recon.CCalcVolThick().DoIt(ts, ap, c["pix"], seed=c["seed"])
+    torch.cuda.synchronize()
+    t = time.perf_counter()
+    for _ in range(args.steps):
+        r = recon.CCalcVolThick().DoIt(ts, ap, c["pix"], seed=c["seed"])
+    torch.cuda.synchronize()
+    ms = (time.perf_counter() - t) / args.steps * 1e3
+    units = float(c["nx"]) * c["ny"] * T
+    line = {"metric": "thickness measurements/s (CCalcVolThick)", "value": 1e3 / ms, "unit": "series/s",
+            "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": c["label"], "name": c["name"]},
+            "e2e": {"value": 1e3 / ms, "unit": "series/s", "h2d_bytes_per_step": int(frames.nbytes),
+                    "d2h_bytes_per_step": 4 * (r.result.vol_z - 1)},
+            "result": {"edges": list(r.m_aiSampleEdges), "thickness": r.result.thickness,
+                       "offset_z": r.result.offset_z, "binning": float(r.m_fBinning)},
+            "raw_gpixel_per_s": units / (ms / 1e3) / 1e9}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -723,7 +940,20 @@ def main():
     ap.add_argument("--inflight", type=int, default=4, help="serve_mix: requests on the GPU at once")
     ap.add_argument("--out-buffers", type=int, default=12, help="serve_mix: pinned host volume buffers")
     ap.add_argument("--hbm-budget-gb", type=float, default=150.0, help="serve_mix: HBM admission budget")
+    ap.add_argument("--tilts", type=int, default=0, help="stack_4k / thick_4k: first N tilts only (0: all)")
     args = ap.parse_args()
+    if args.workload in ("stack_4k", "thick_4k"):
+        if args.impl == "reference":
+            c = stack_workload(args.workload)
+            base = stack_cpu_baseline(c, synth_frames(c))
+            print(json.dumps({"impl": "reference", "metric": STACK_METRIC, "value": base["value"], "unit": STACK_UNIT,
+                              "n_gpus": 1, "steps": 1, "warmup": 0, "higher_is_better": True, "dtype": "f64",
+                              "config": {"workload": c["label"], "name": c["name"]}, "cpu_baseline": base,
+                              "e2e": {"value": base["value"], "unit": STACK_UNIT, "h2d_bytes_per_step": 0,
+                                      "d2h_bytes_per_step": 0}}), flush=True)
+        else:
+            run_stack_arm(args)
+        return
     if args.impl == "ours" and args.workload in ("batch_uneven", "serve_mix"):
         if args.workload == "batch_uneven":
             run_batch_arm(args)

@@ -4,7 +4,7 @@
 // target for the input-stage and thickness tests; nothing in the product
 // links or calls it.
 //
-//   ref_stack stack <in.bin> <params.bin> <out.bin> <seed> <bin> <size_axis>
+//   ref_stack stack <in.bin> <params.bin> <out.bin> <seed> <bin> <size_axis> [noaligned]
 //     As CCorrTomoStack::DoIt / mCorrectProj run every tilt with Fourier
 //     cropping (AreTomo/Correct/CCorrTomoStack.cpp:164-222): GCorrPatchShift
 //     (shift, rotation, local patches, random fill) into the padded aligned
@@ -12,6 +12,8 @@
 //     inverse 2-D FFT of CFourierCropImage::mCropFFT (or its mCopy when the
 //     sizes agree), unpadded.  The fill's random table is seeded with `seed`:
 //     this driver defines time() to return it, which GGenRandoms::DoIt reads.
+//     `noaligned` skips the copy-out of the aligned frames (not part of
+//     CCorrTomoStack::DoIt), for timing; out.bin then has no aligned block.
 //     in.bin    : int32 nx, ny, T; float32 tilts[T]; float32 frames[T][ny][nx]
 //     params.bin: int32 P, shift_only; float32 shifts[T][2]; float32 axes[T];
 //                 float32 local[T][5][P]
@@ -87,6 +89,7 @@ static int run_stack(int argc, char** argv)
     fclose(fp);
     g_seed = (time_t)strtoll(argv[5], nullptr, 10);
     const float bin = (float)atof(argv[6]), size_axis = (float)atof(argv[7]);
+    const bool keep_aligned = !(argc > 8 && std::string(argv[8]) == "noaligned");
 
     int raw_size[2] = {nx, ny}, aln[2] = {0, 0}, bnd[2] = {0, 0};
     MAC::CCorrectUtil::CalcAlignedSize(raw_size, size_axis, aln);
@@ -99,7 +102,7 @@ static int run_stack(int argc, char** argv)
     cudaMalloc(&g_bin, sizeof(float) * (size_t)std::max(bin_pad[0] * bin_pad[1], aln_pad[0] * aln_pad[1]));
     cudaMemset(g_corr, 0, sizeof(float) * aln_pad[0] * aln_pad[1]);
     if (P > 0) cudaMalloc(&g_local, sizeof(float) * 5 * P);
-    std::vector<float> aligned((size_t)nt * aln[0] * aln[1]), binned((size_t)nt * bnd[0] * bnd[1]);
+    std::vector<float> aligned(keep_aligned ? (size_t)nt * aln[0] * aln[1] : 0), binned((size_t)nt * bnd[0] * bnd[1]);
     std::vector<int> table;
     cudaDeviceSynchronize();
     auto t0 = std::chrono::steady_clock::now();
@@ -122,7 +125,7 @@ static int run_stack(int argc, char** argv)
             float shift[2] = {shifts[2 * t], shifts[2 * t + 1]};
             const float axis = shift_only ? 0.0f : axes[t];
             corr.DoIt(g_raw, shift, axis, g_local, true, g_corr);
-            pad.Unpad(g_corr, aln_pad, aligned.data() + (size_t)t * aln[0] * aln[1]);
+            if (keep_aligned) pad.Unpad(g_corr, aln_pad, aligned.data() + (size_t)t * aln[0] * aln[1]);
             if (same) {
                 pad.Unpad(g_corr, aln_pad, binned.data() + (size_t)t * bnd[0] * bnd[1]);
                 continue;
