@@ -731,13 +731,15 @@ at3r_status at3r_run_device(at3r_plan* p, const float* proj, float* vol, void* s
     return end_run(p, st);
 }
 
+}  // extern "C"
+
+namespace at3r {
+
 // Host <-> device staging for pageable caller memory.  A copy between the
 // device and pageable host memory runs at a fraction of the link's rate (the
 // driver stages it itself, synchronously); instead, data passes through two
 // pinned 64 MB ring slots, and the host side of each slot (pageable <->
 // pinned) is a parallel memcpy that overlaps the GPU's work.
-constexpr size_t kStageBytes = (size_t)64 << 20;
-
 bool host_pinned(const void* ptr)
 {
     cudaPointerAttributes a{};
@@ -747,12 +749,6 @@ bool host_pinned(const void* ptr)
     }
     return a.type == cudaMemoryTypeHost;
 }
-
-struct Piece {
-    char* dst;
-    const char* src;
-    size_t bytes;
-};
 
 // memcpy of every piece, split over up to 8 host threads (4 MB or more each)
 void parallel_copy(const std::vector<Piece>& pieces)
@@ -795,8 +791,8 @@ std::vector<Piece> split_pieces(const std::vector<Piece>& in)
 // a run borrows one and returns it, so plans created per series do not pay
 // for pinned allocations (256 MB of cudaHostAlloc took longer than a 512^3
 // WBP).  The pool grows to the number of runs in flight at once.
-std::mutex g_stage_mu;
-std::vector<char*> g_stage_free;   // each entry: 4 * kStageBytes pinned
+static std::mutex g_stage_mu;
+static std::vector<char*> g_stage_free;   // each entry: 4 * kStageBytes pinned
 
 char* stage_acquire()
 {
@@ -823,7 +819,6 @@ void stage_release(char* s)
     g_stage_free.push_back(s);
 }
 
-// Borrows a staging set for this run; the caller returns it with stage_return.
 // Consecutive pieces whose source and destination both continue where the
 // previous one ended, merged into one (fewer, larger copies).
 std::vector<Piece> merge_pieces(const std::vector<Piece>& in)
@@ -838,6 +833,11 @@ std::vector<Piece> merge_pieces(const std::vector<Piece>& in)
     return out;
 }
 
+}  // namespace at3r
+
+extern "C" {
+
+// Borrows a staging set for this run; the caller returns it with stage_return.
 at3r_status ensure_stage(at3r_plan* p)
 {
     char* s = stage_acquire();

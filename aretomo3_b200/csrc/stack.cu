@@ -39,8 +39,13 @@ struct at3r_stack {
     uint8_t* d_empty = nullptr;    // [chunk][W * ay]
     float2* d_Y = nullptr;         // [chunk][ay][KXo]
     float2* d_Wc = nullptr;        // [chunk][by][KXo]
-    float* d_raw = nullptr;        // host path: [chunk][ny][nx]
-    float* d_out = nullptr;        // host path: [chunk][by][bx]
+    // host path: two buffers of hc tilts each, raw in and binned out, on
+    // their own copy streams (double-buffered against the compute stream)
+    int hc = 0;
+    float* d_raw2[2] = {nullptr, nullptr};
+    float* d_out2[2] = {nullptr, nullptr};
+    cudaStream_t s_in = nullptr, s_out = nullptr;
+    cudaEvent_t ev_in[2] = {}, ev_comp[2] = {}, ev_outdone[2] = {}, ev_slot[4] = {};
     HostFft frow, fcin, fcout, fbx;
     int b_row = 1, b_c2r = 1, cb = 1, col_pitch = 0, rs_col = 0;
     size_t smem_row = 0, smem_col = 0, smem_c2r = 0;
@@ -183,6 +188,130 @@ at3r_status check_device(const at3r_stack* s)
     return AT3R_OK;
 }
 
+// Host-path buffers and streams, made on first use: chunks of about 256 MB
+// of raw frames (at least one tilt, at most a device pass).
+at3r_status ensure_host_path(at3r_stack* s)
+{
+    if (s->hc) return AT3R_OK;
+    const size_t fin = (size_t)s->nx * s->ny * sizeof(float);
+    const int hc = (int)std::max<size_t>(1, std::min<size_t>((size_t)s->chunk, (256ull << 20) / fin));
+    at3r_status rc;
+    for (int b = 0; b < 2; b++)
+        if ((rc = salloc(&s->d_raw2[b], (size_t)hc * s->nx * s->ny)) ||
+            (rc = salloc(&s->d_out2[b], (size_t)hc * s->bx * s->by)))
+            return rc;
+    ST_CUDA(cudaStreamCreateWithFlags(&s->s_in, cudaStreamNonBlocking));
+    ST_CUDA(cudaStreamCreateWithFlags(&s->s_out, cudaStreamNonBlocking));
+    for (cudaEvent_t* e : {&s->ev_in[0], &s->ev_in[1], &s->ev_comp[0], &s->ev_comp[1], &s->ev_outdone[0],
+                           &s->ev_outdone[1], &s->ev_slot[0], &s->ev_slot[1], &s->ev_slot[2], &s->ev_slot[3]})
+        ST_CUDA(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+    s->hc = hc;
+    return AT3R_OK;
+}
+
+// Copies between pageable host frames and the device through the four
+// pinned slots of a staging set: slots 0 and 1 carry frames in (a parallel
+// host memcpy into a slot, then its copy to the device on s_in), slots 2 and 3
+// carry binned frames out (a copy from the device on s_out; the host memcpy
+// out of the slot runs when the slot is next needed, or at the end), so host
+// copies overlap the GPU's copies and passes.
+struct Stager {
+    at3r_stack* s;
+    char* set;
+    int in_slot = 0, out_slot = 0;
+    std::vector<Piece> pending[2];   // host copies still owed by out slots 0 / 1
+
+    char* slot(int i) const { return set + (size_t)i * kStageBytes; }
+
+    at3r_status direct(const std::vector<Piece>& pcs, cudaMemcpyKind kind, cudaStream_t strm)
+    {
+        for (const Piece& pc : merge_pieces(pcs)) ST_CUDA(cudaMemcpyAsync(pc.dst, pc.src, pc.bytes, kind, strm));
+        return AT3R_OK;
+    }
+
+    at3r_status in(const std::vector<Piece>& pcs)
+    {
+        std::vector<Piece> group;
+        size_t used = 0;
+        auto flush = [&]() -> at3r_status {
+            if (group.empty()) return AT3R_OK;
+            ST_CUDA(cudaEventSynchronize(s->ev_slot[in_slot]));
+            char* sl = slot(in_slot);
+            std::vector<Piece> host, dev;
+            size_t o = 0;
+            for (const Piece& pc : group) {
+                host.push_back({sl + o, pc.src, pc.bytes});
+                dev.push_back({pc.dst, sl + o, pc.bytes});
+                o += pc.bytes;
+            }
+            parallel_copy(host);
+            for (const Piece& pc : merge_pieces(dev))
+                ST_CUDA(cudaMemcpyAsync(pc.dst, pc.src, pc.bytes, cudaMemcpyHostToDevice, s->s_in));
+            ST_CUDA(cudaEventRecord(s->ev_slot[in_slot], s->s_in));
+            in_slot ^= 1;
+            group.clear();
+            used = 0;
+            return AT3R_OK;
+        };
+        at3r_status rc;
+        for (const Piece& pc : split_pieces(pcs)) {
+            if (used + pc.bytes > kStageBytes && (rc = flush())) return rc;
+            group.push_back(pc);
+            used += pc.bytes;
+        }
+        return flush();
+    }
+
+    at3r_status drain(int k)
+    {
+        if (pending[k].empty()) return AT3R_OK;
+        ST_CUDA(cudaEventSynchronize(s->ev_slot[2 + k]));
+        parallel_copy(pending[k]);
+        pending[k].clear();
+        return AT3R_OK;
+    }
+
+    at3r_status out(const std::vector<Piece>& pcs)
+    {
+        std::vector<Piece> group;
+        size_t used = 0;
+        at3r_status rc;
+        auto flush = [&]() -> at3r_status {
+            if (group.empty()) return AT3R_OK;
+            if ((rc = drain(out_slot))) return rc;
+            char* sl = slot(2 + out_slot);
+            std::vector<Piece> dev;
+            size_t o = 0;
+            for (const Piece& pc : group) {
+                dev.push_back({sl + o, pc.src, pc.bytes});
+                pending[out_slot].push_back({pc.dst, sl + o, pc.bytes});
+                o += pc.bytes;
+            }
+            for (const Piece& pc : merge_pieces(dev))
+                ST_CUDA(cudaMemcpyAsync(pc.dst, pc.src, pc.bytes, cudaMemcpyDeviceToHost, s->s_out));
+            ST_CUDA(cudaEventRecord(s->ev_slot[2 + out_slot], s->s_out));
+            out_slot ^= 1;
+            group.clear();
+            used = 0;
+            return AT3R_OK;
+        };
+        for (const Piece& pc : split_pieces(pcs)) {
+            if (used + pc.bytes > kStageBytes && (rc = flush())) return rc;
+            group.push_back(pc);
+            used += pc.bytes;
+        }
+        return flush();
+    }
+
+    at3r_status drain_all()
+    {
+        at3r_status rc;
+        // the older slot first, so the frames land in order
+        if ((rc = drain(out_slot)) || (rc = drain(out_slot ^ 1))) return rc;
+        return AT3R_OK;
+    }
+};
+
 // CCalcVolThick::mSmooth (CCalcVolThick.cpp:114-132): 11-sample box filter,
 // indices clamped at the ends, sums in double.
 void smooth_profile(std::vector<float>& cc)
@@ -252,6 +381,152 @@ void detect_edges(const std::vector<float>& cc, float bin, at3r_thickness* r)
     r->offset_z = (e0 + e1) / 2 - (int)(half * bin);
 }
 
+
+// The host path: tilt chunks of s->hc frames double-buffered over the copy
+// streams and the compute stream.  Binned frames go to binned_frames (host)
+// or, with binned_dev, stay on the device at binned_dev[T][by][bx].
+at3r_status stack_pipeline(at3r_stack* s, const float* const* frames, float* const* binned_frames, float* binned_dev,
+                           void* stream)
+{
+    at3r_status rc;
+    const size_t fin = (size_t)s->nx * s->ny * sizeof(float), fout = (size_t)s->bx * s->by * sizeof(float);
+    if ((rc = ensure_host_path(s))) return rc;
+    bool pin_in = true, pin_out = true;
+    for (int t = 0; t < s->T && (pin_in || pin_out); t++) {
+        pin_in = pin_in && host_pinned(frames[t]);
+        pin_out = pin_out && (binned_dev || host_pinned(binned_frames[t]));
+    }
+    char* stage = nullptr;
+    if (!(pin_in && pin_out) && !(stage = stage_acquire()))
+        return st_err(AT3R_ERR_OUT_OF_MEMORY, "pinned staging allocation failed");
+    cudaStream_t st = (cudaStream_t)stream;
+    Stager sg{s, stage};
+    auto body = [&]() -> at3r_status {
+        const int hc = s->hc;
+        for (int k = 0, t0 = 0; t0 < s->T; k++, t0 += hc) {
+            const int n = std::min(hc, s->T - t0), b = k & 1;
+            // raw frames in, once the pass two chunks back has read this buffer
+            if (k >= 2) ST_CUDA(cudaStreamWaitEvent(s->s_in, s->ev_comp[b], 0));
+            std::vector<Piece> in;
+            for (int j = 0; j < n; j++)
+                in.push_back({reinterpret_cast<char*>(s->d_raw2[b]) + j * fin,
+                              reinterpret_cast<const char*>(frames[t0 + j]), fin});
+            if ((rc = pin_in ? sg.direct(in, cudaMemcpyHostToDevice, s->s_in) : sg.in(in))) return rc;
+            ST_CUDA(cudaEventRecord(s->ev_in[b], s->s_in));
+            // the pass, once its frames are in and this output buffer went out
+            ST_CUDA(cudaStreamWaitEvent(st, s->ev_in[b], 0));
+            if (k >= 2) ST_CUDA(cudaStreamWaitEvent(st, s->ev_outdone[b], 0));
+            float* dst = binned_dev ? binned_dev + (size_t)t0 * s->bx * s->by : s->d_out2[b];
+            if ((rc = run_chunk(s, s->d_raw2[b], t0, n, dst, st))) return rc;
+            ST_CUDA(cudaEventRecord(s->ev_comp[b], st));
+            if (binned_dev) continue;
+            // binned frames out
+            ST_CUDA(cudaStreamWaitEvent(s->s_out, s->ev_comp[b], 0));
+            std::vector<Piece> out;
+            for (int j = 0; j < n; j++)
+                out.push_back({reinterpret_cast<char*>(binned_frames[t0 + j]),
+                               reinterpret_cast<const char*>(s->d_out2[b]) + j * fout, fout});
+            if ((rc = pin_out ? sg.direct(out, cudaMemcpyDeviceToHost, s->s_out) : sg.out(out))) return rc;
+            ST_CUDA(cudaEventRecord(s->ev_outdone[b], s->s_out));
+        }
+        if ((rc = sg.drain_all())) return rc;
+        ST_CUDA(cudaStreamSynchronize(s->s_out));
+        ST_CUDA(cudaStreamSynchronize(st));
+        return AT3R_OK;
+    };
+    rc = body();
+    if (rc) {
+        cudaStreamSynchronize(s->s_in);
+        cudaStreamSynchronize(s->s_out);
+        cudaStreamSynchronize(st);
+        cudaGetLastError();
+    }
+    stage_release(stage);
+    return rc;
+}
+
+// CCalcVolThick::DoIt on a device-resident (raw) or host (frames) series.
+at3r_status thickness_impl(const at3r_stack_geom* g, const float* tilts_deg, float pix_size, const float* raw,
+                           const float* const* frames, float* profile, float* profile_smoothed, int profile_cap,
+                           at3r_thickness* res, void* stream)
+{
+    if (!g || !tilts_deg || !(raw || frames) || !res) return st_err(AT3R_ERR_INVALID_ARGUMENT, "null argument");
+    if (!(pix_size > 0.f)) return st_err(AT3R_ERR_INVALID_ARGUMENT, "pixel size must be > 0");
+    std::memset(res, 0, sizeof(*res));
+    cudaStream_t st = (cudaStream_t)stream;
+    // CCalcVolThick::DoIt: binning max(20 A / pixel, 20), Fourier crop with
+    // random fill, rotation by the tilt axis, no local patches
+    at3r_stack_geom h = *g;
+    h.correct = 1;
+    h.rand_fill = 1;
+    h.num_patches = 0;
+    h.local_params = nullptr;
+    h.bin = std::fmax(20.0f / pix_size, 20.0f);
+    res->binning = h.bin;
+    at3r_stack* s = nullptr;
+    at3r_status rc = at3r_stack_create(&h, &s);
+    if (rc) return rc;
+    const int bx = s->bx, by = s->by, T = s->T;
+    res->binned_xy[0] = bx;
+    res->binned_xy[1] = by;
+    const int vol_z = (int)(bx * 0.8) / 2 * 2;
+    res->vol_z = vol_z;
+    const int n = vol_z - 1;
+    if (n < 10 || bx < 4) {
+        at3r_stack_destroy(s);
+        return st_err(AT3R_ERR_INVALID_ARGUMENT, "series too small for the thickness measurement after binning by " +
+                                                     std::to_string(h.bin));
+    }
+    float* binned = nullptr;
+    float* vol = nullptr;
+    float* d_prof = nullptr;
+    at3r_plan* plan = nullptr;
+    auto cleanup = [&](at3r_status r) {
+        if (plan) at3r_plan_destroy(plan);
+        cudaStreamSynchronize(st);
+        for (void* p : {(void*)binned, (void*)vol, (void*)d_prof})
+            if (p) cudaFree(p);
+        at3r_stack_destroy(s);
+        return r;
+    };
+    if ((rc = salloc(&binned, (size_t)T * bx * by))) return cleanup(rc);
+    if ((rc = raw ? at3r_stack_run_device(s, raw, binned, stream)
+                  : stack_pipeline(s, frames, nullptr, binned, stream)))
+        return cleanup(rc);
+    // low-resolution WBP (CDoWbpRecon::DoIt) of the binned series
+    at3r_geom wg;
+    at3r_geom_init(&wg, AT3R_WBP);
+    wg.nx = bx;
+    wg.ny = by;
+    wg.n_tilts = T;
+    wg.tilts_deg = tilts_deg;
+    wg.vol_z = vol_z;
+    if ((rc = at3r_plan_create(&wg, &plan))) return cleanup(rc);
+    const int Nx = bx & ~1;
+    if ((rc = salloc(&vol, (size_t)by * vol_z * Nx))) return cleanup(rc);
+    if ((rc = at3r_run_device(plan, binned, vol, stream))) return cleanup(rc);
+    // plane statistics of FlipVol(true) (CCalcVolThick.cpp:85-103, 172-197,
+    // 199-206): tile 40 % of x and y (even), centred in x; its rows start at
+    // row 0 because mMeasureStd indexes row j, not start + j
+    const int tx = (int)(Nx * 0.4f) / 2 * 2, ty = (int)(by * 0.4f) / 2 * 2;
+    const int x0 = (Nx - tx) / 2;
+    if ((rc = salloc(&d_prof, (size_t)n))) return cleanup(rc);
+    k_plane_std<<<n, 256, 0, st>>>(vol, Nx, vol_z, x0, 0, tx, ty, d_prof);
+    std::vector<float> cc(n);
+    if (cudaGetLastError() != cudaSuccess ||
+        cudaMemcpyAsync(cc.data(), d_prof, sizeof(float) * n, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess) {
+        cudaGetLastError();
+        return cleanup(st_err(AT3R_ERR_CUDA, "plane statistics failed"));
+    }
+    if (profile) std::memcpy(profile, cc.data(), sizeof(float) * std::min(n, std::max(profile_cap, 0)));
+    smooth_profile(cc);
+    if (profile_smoothed) std::memcpy(profile_smoothed, cc.data(), sizeof(float) * std::min(n, std::max(profile_cap, 0)));
+    detect_edges(cc, h.bin, res);
+    res->n_profile = n;
+    return cleanup(AT3R_OK);
+}
+
 }  // namespace
 
 extern "C" {
@@ -273,10 +548,15 @@ void at3r_stack_destroy(at3r_stack* s)
     if (cur != s->device) cudaSetDevice(s->device);
     cudaDeviceSynchronize();
     for (void* p : {(void*)s->d_shift, (void*)s->d_cs, (void*)s->d_local, (void*)s->d_rand, (void*)s->d_flags,
-                    (void*)s->d_aln, (void*)s->d_empty, (void*)s->d_Y, (void*)s->d_Wc, (void*)s->d_raw,
-                    (void*)s->d_out, (void*)s->frow.d_tables, (void*)s->fcin.d_tables, (void*)s->fcout.d_tables,
-                    (void*)s->fbx.d_tables})
+                    (void*)s->d_aln, (void*)s->d_empty, (void*)s->d_Y, (void*)s->d_Wc, (void*)s->d_raw2[0],
+                    (void*)s->d_raw2[1], (void*)s->d_out2[0], (void*)s->d_out2[1], (void*)s->frow.d_tables,
+                    (void*)s->fcin.d_tables, (void*)s->fcout.d_tables, (void*)s->fbx.d_tables})
         if (p) cudaFree(p);
+    for (cudaEvent_t* e : {&s->ev_in[0], &s->ev_in[1], &s->ev_comp[0], &s->ev_comp[1], &s->ev_outdone[0],
+                           &s->ev_outdone[1], &s->ev_slot[0], &s->ev_slot[1], &s->ev_slot[2], &s->ev_slot[3]})
+        if (*e) cudaEventDestroy(*e);
+    if (s->s_in) cudaStreamDestroy(s->s_in);
+    if (s->s_out) cudaStreamDestroy(s->s_out);
     cudaGetLastError();
     if (cur >= 0 && cur != s->device) cudaSetDevice(cur);
     delete s;
@@ -391,7 +671,6 @@ at3r_status at3r_stack_create(const at3r_stack_geom* g, at3r_stack** out)
     size_t per_tilt = 0;
     if (g->correct) per_tilt += sizeof(float) * (size_t)s->ax * s->ay + (g->rand_fill ? (size_t)s->W * s->ay : 0);
     if (!s->same) per_tilt += sizeof(float2) * (size_t)s->KXo * (s->ay + s->by);
-    per_tilt += sizeof(float) * ((size_t)s->nx * s->ny + (size_t)s->bx * s->by);   // host-path frames
     s->chunk = (int)std::max<size_t>(1, std::min<size_t>(T, (size_t)(8ull << 30) / std::max<size_t>(per_tilt, 1)));
     const size_t C = s->chunk;
     if (g->correct) {
@@ -456,99 +735,15 @@ at3r_status at3r_stack_run_host(at3r_stack* s, const float* const* frames, float
     if ((rc = check_device(s))) return rc;
     for (int t = 0; t < s->T; t++)
         if (!frames[t] || !binned_frames[t]) return st_err(AT3R_ERR_INVALID_ARGUMENT, "null frame pointer");
-    const size_t C = s->chunk, fin = (size_t)s->nx * s->ny, fout = (size_t)s->bx * s->by;
-    if (!s->d_raw && ((rc = salloc(&s->d_raw, C * fin)) || (rc = salloc(&s->d_out, C * fout)))) return rc;
-    cudaStream_t st = (cudaStream_t)stream;
-    for (int t0 = 0; t0 < s->T; t0 += s->chunk) {
-        const int n = std::min(s->chunk, s->T - t0);
-        for (int k = 0; k < n; k++)
-            ST_CUDA(cudaMemcpyAsync(s->d_raw + k * fin, frames[t0 + k], sizeof(float) * fin, cudaMemcpyHostToDevice, st));
-        if ((rc = run_chunk(s, s->d_raw, t0, n, s->d_out, st))) return rc;
-        for (int k = 0; k < n; k++)
-            ST_CUDA(cudaMemcpyAsync(binned_frames[t0 + k], s->d_out + k * fout, sizeof(float) * fout,
-                                    cudaMemcpyDeviceToHost, st));
-    }
-    ST_CUDA(cudaStreamSynchronize(st));
-    return AT3R_OK;
+    return stack_pipeline(s, frames, binned_frames, nullptr, stream);
 }
 
 at3r_status at3r_thickness_device(const at3r_stack_geom* g, const float* tilts_deg, float pix_size, const float* raw,
                                   float* profile, float* profile_smoothed, int profile_cap, at3r_thickness* res,
                                   void* stream)
 {
-    if (!g || !tilts_deg || !raw || !res) return st_err(AT3R_ERR_INVALID_ARGUMENT, "null argument");
-    if (!(pix_size > 0.f)) return st_err(AT3R_ERR_INVALID_ARGUMENT, "pixel size must be > 0");
-    std::memset(res, 0, sizeof(*res));
-    cudaStream_t st = (cudaStream_t)stream;
-    // CCalcVolThick::DoIt: binning max(20 A / pixel, 20), Fourier crop with
-    // random fill, rotation by the tilt axis, no local patches
-    at3r_stack_geom h = *g;
-    h.correct = 1;
-    h.rand_fill = 1;
-    h.num_patches = 0;
-    h.local_params = nullptr;
-    h.bin = std::fmax(20.0f / pix_size, 20.0f);
-    res->binning = h.bin;
-    at3r_stack* s = nullptr;
-    at3r_status rc = at3r_stack_create(&h, &s);
-    if (rc) return rc;
-    const int bx = s->bx, by = s->by, T = s->T;
-    res->binned_xy[0] = bx;
-    res->binned_xy[1] = by;
-    const int vol_z = (int)(bx * 0.8) / 2 * 2;
-    res->vol_z = vol_z;
-    const int n = vol_z - 1;
-    if (n < 10 || bx < 4) {
-        at3r_stack_destroy(s);
-        return st_err(AT3R_ERR_INVALID_ARGUMENT, "series too small for the thickness measurement after binning by " +
-                                                     std::to_string(h.bin));
-    }
-    float* binned = nullptr;
-    float* vol = nullptr;
-    float* d_prof = nullptr;
-    at3r_plan* plan = nullptr;
-    auto cleanup = [&](at3r_status r) {
-        if (plan) at3r_plan_destroy(plan);
-        cudaStreamSynchronize(st);
-        for (void* p : {(void*)binned, (void*)vol, (void*)d_prof})
-            if (p) cudaFree(p);
-        at3r_stack_destroy(s);
-        return r;
-    };
-    if ((rc = salloc(&binned, (size_t)T * bx * by))) return cleanup(rc);
-    if ((rc = at3r_stack_run_device(s, raw, binned, stream))) return cleanup(rc);
-    // low-resolution WBP (CDoWbpRecon::DoIt) of the binned series
-    at3r_geom wg;
-    at3r_geom_init(&wg, AT3R_WBP);
-    wg.nx = bx;
-    wg.ny = by;
-    wg.n_tilts = T;
-    wg.tilts_deg = tilts_deg;
-    wg.vol_z = vol_z;
-    if ((rc = at3r_plan_create(&wg, &plan))) return cleanup(rc);
-    const int Nx = bx & ~1;
-    if ((rc = salloc(&vol, (size_t)by * vol_z * Nx))) return cleanup(rc);
-    if ((rc = at3r_run_device(plan, binned, vol, stream))) return cleanup(rc);
-    // plane statistics of FlipVol(true) (CCalcVolThick.cpp:85-103, 172-197,
-    // 199-206): tile 40 % of x and y (even), centred in x; its rows start at
-    // row 0 because mMeasureStd indexes row j, not start + j
-    const int tx = (int)(Nx * 0.4f) / 2 * 2, ty = (int)(by * 0.4f) / 2 * 2;
-    const int x0 = (Nx - tx) / 2;
-    if ((rc = salloc(&d_prof, (size_t)n))) return cleanup(rc);
-    k_plane_std<<<n, 256, 0, st>>>(vol, Nx, vol_z, x0, 0, tx, ty, d_prof);
-    std::vector<float> cc(n);
-    if (cudaGetLastError() != cudaSuccess ||
-        cudaMemcpyAsync(cc.data(), d_prof, sizeof(float) * n, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
-        cudaStreamSynchronize(st) != cudaSuccess) {
-        cudaGetLastError();
-        return cleanup(st_err(AT3R_ERR_CUDA, "plane statistics failed"));
-    }
-    if (profile) std::memcpy(profile, cc.data(), sizeof(float) * std::min(n, std::max(profile_cap, 0)));
-    smooth_profile(cc);
-    if (profile_smoothed) std::memcpy(profile_smoothed, cc.data(), sizeof(float) * std::min(n, std::max(profile_cap, 0)));
-    detect_edges(cc, h.bin, res);
-    res->n_profile = n;
-    return cleanup(AT3R_OK);
+    if (!raw) return st_err(AT3R_ERR_INVALID_ARGUMENT, "null argument");
+    return thickness_impl(g, tilts_deg, pix_size, raw, nullptr, profile, profile_smoothed, profile_cap, res, stream);
 }
 
 at3r_status at3r_thickness_host(const at3r_stack_geom* g, const float* tilts_deg, float pix_size,
@@ -559,22 +754,7 @@ at3r_status at3r_thickness_host(const at3r_stack_geom* g, const float* tilts_deg
     if (g->nx < 2 || g->ny < 2 || g->n_tilts < 1) return st_err(AT3R_ERR_INVALID_ARGUMENT, "invalid sizes");
     for (int t = 0; t < g->n_tilts; t++)
         if (!frames[t]) return st_err(AT3R_ERR_INVALID_ARGUMENT, "null frame pointer");
-    const size_t frame = (size_t)g->nx * g->ny;
-    float* raw = nullptr;
-    at3r_status rc;
-    if ((rc = salloc(&raw, frame * g->n_tilts))) return rc;
-    cudaStream_t st = (cudaStream_t)stream;
-    for (int t = 0; t < g->n_tilts; t++)
-        if (cudaMemcpyAsync(raw + t * frame, frames[t], sizeof(float) * frame, cudaMemcpyHostToDevice, st) !=
-            cudaSuccess) {
-            cudaGetLastError();
-            cudaFree(raw);
-            return st_err(AT3R_ERR_CUDA, "frame upload failed");
-        }
-    rc = at3r_thickness_device(g, tilts_deg, pix_size, raw, profile, profile_smoothed, profile_cap, res, stream);
-    cudaStreamSynchronize(st);
-    cudaFree(raw);
-    return rc;
+    return thickness_impl(g, tilts_deg, pix_size, nullptr, frames, profile, profile_smoothed, profile_cap, res, stream);
 }
 
 }  // extern "C"

@@ -80,6 +80,33 @@ def test_device_path_equals_host_path():
         st.close()
 
 
+def test_host_pipeline_over_several_chunks():
+    # 64 MB frames: the host path moves four tilts per chunk, double-buffered,
+    # through the pinned staging slots (pageable frames) or directly (pinned)
+    import torch
+    rng = np.random.default_rng(15)
+    T, ny, nx = 9, 4096, 4096
+    frames = rng.standard_normal((T, ny, nx), dtype=np.float32)
+    st = recon.Stack(nx, ny, T, shifts=rng.uniform(-9, 9, (T, 2)), tilt_axes=rng.uniform(85, 87, T), size_axis=86.0,
+                     seed=2, bin=4.0)
+    try:
+        raw = torch.from_numpy(frames).cuda()
+        out = torch.empty(st.binned_shape, device="cuda", dtype=torch.float32)
+        st.run_device(raw.data_ptr(), out.data_ptr(), torch.cuda.current_stream().cuda_stream)
+        torch.cuda.synchronize()
+        dev = out.cpu().numpy()
+        assert np.array_equal(st.run_host([f for f in frames]), dev)
+        pin_in = torch.from_numpy(frames).pin_memory()
+        pin_out = torch.empty(st.binned_shape, dtype=torch.float32).pin_memory()
+        st.run_host([pin_in[t].numpy() for t in range(T)], pin_out.numpy())
+        assert np.array_equal(pin_out.numpy(), dev)
+        mixed = np.empty(st.binned_shape, np.float32)
+        st.run_host([pin_in[t].numpy() for t in range(T)], mixed)
+        assert np.array_equal(mixed, dev)
+    finally:
+        st.close()
+
+
 @pytest.mark.parametrize("nx,ny,T,bin,axes", [(1000, 1022, 5, 4.0, (-3.0, 3.0)), (1024, 768, 4, 2.0, (85.0, 87.0)),
                                               (510, 498, 3, 1.7, (0.0, 0.0)), (1000, 1022, 4, 4.0, (0.0, 0.0))])
 def test_stack_matches_oracle_larger(nx, ny, T, bin, axes):
