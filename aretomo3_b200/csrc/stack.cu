@@ -27,6 +27,7 @@ struct at3r_stack {
     int bx = 0, by = 0, KXo = 0;   // binned frame; kept row bins
     bool same = false;             // binned size == aligned size: no Fourier crop
     int P = 0;                     // local-alignment patches
+    int by_rows = 0;               // k_corr visits tiles along aligned y (axis nearer 90 than 0 degrees)
     int chunk = 1;                 // tilts per device pass
     int c2r = AT3R_C2R_HERMITIAN;
     float norm = 1.f;
@@ -146,14 +147,16 @@ at3r_status run_chunk(at3r_stack* s, const float* raw, int t0, int n, float* out
     const float* src = raw;
     if (s->g.correct) {
         const int fill = s->g.rand_fill ? 1 : 0;
-        k_corr<<<dim3((s->ax + 31) / 32, (s->ay + 7) / 8, n), 256, 0, st>>>(
-            raw, s->nx, s->ny, s->ax, s->ay, s->W, s->d_shift + t0, s->d_cs + t0,
-            s->d_local ? s->d_local + (size_t)t0 * 5 * s->P : nullptr, s->P, fill, s->d_aln, s->d_empty);
+        const dim3 grid = s->by_rows ? dim3((s->ay + 31) / 32, (s->ax + 31) / 32, n)
+                                     : dim3((s->ax + 31) / 32, (s->ay + 31) / 32, n);
+        k_corr<<<grid, 256, 0, st>>>(raw, s->nx, s->ny, s->ax, s->ay, s->W, s->d_shift + t0, s->d_cs + t0,
+                                     s->d_local ? s->d_local + (size_t)t0 * 5 * s->P : nullptr, s->P, fill,
+                                     s->by_rows, s->d_aln, s->d_empty);
         ST_CUDA(cudaGetLastError());
         if (fill) {
             ST_CUDA(cudaMemsetAsync(s->d_flags, 0, sizeof(int) * n, st));
             const int npx = s->W * s->ay;
-            k_fill<<<dim3((npx + 255) / 256, n), 256, 0, st>>>(s->d_aln, s->d_empty, s->d_rand, s->W, s->ax, s->ay,
+            k_fill<<<dim3((npx + 1023) / 1024, n), 256, 0, st>>>(s->d_aln, s->d_empty, s->d_rand, s->W, s->ax, s->ay,
                                                                s->d_flags);
             k_fill_mean<<<n, 512, 0, st>>>(s->d_aln, s->d_empty, s->W, s->ax, s->ay, s->d_flags);
             ST_CUDA(cudaGetLastError());
@@ -615,6 +618,12 @@ at3r_status at3r_stack_create(const at3r_stack_geom* g, at3r_stack** out)
         std::vector<float> rad(T, 0.f);
         if (g->tilt_axes_deg)
             for (size_t t = 0; t < T; t++) rad[t] = g->tilt_axes_deg[t] * d2r;
+        double sum_c = 0.0, sum_s = 0.0;
+        for (size_t t = 0; t < T; t++) {
+            sum_c += std::fabs(std::cos((double)rad[t]));
+            sum_s += std::fabs(std::sin((double)rad[t]));
+        }
+        s->by_rows = sum_s > sum_c ? 1 : 0;
         float* d_rad = nullptr;
         if ((rc = salloc(&s->d_shift, T)) || (rc = salloc(&s->d_cs, T)) || (rc = salloc(&d_rad, T)))
             return fail(rc);

@@ -46,40 +46,21 @@ __global__ void k_axis_cs(const float* __restrict__ rad, int T, float2* __restri
     if (t < T) cs[t] = make_float2(cosf(rad[t]), sinf(rad[t]));
 }
 
-// GCorrPatchShift.cu:61-104 (mGCorrect) with the local shift of :18-49.
-// Pixel (X, Y) of aligned frame t: centred coordinates rotated by the tilt
-// axis, moved by the weighted patch shift and the global shift, then the
-// nearest raw pixel (int() truncation of coordinate + 0.5), or -1e30 outside
-// the raw frame.  Columns X >= W (the odd-width case) are 0.  With `fill`,
-// the empty mask of the fill is written alongside.
-// local: [T][5][P] = patch centre x, centre y, shift x, shift y, good flag.
-// A CTA covers a 32 x 8 tile, each warp an 8 x 4 patch of it, so that the
-// raw pixels a warp gathers lie within a few rows and columns whatever the
-// rotation (a 32 x 1 warp on a frame rotated by ~90 degrees would read 32 raw
-// rows).  Grid (ceil(ax / 32), ceil(ay / 8), T), 256 threads.
-__global__ void __launch_bounds__(256) k_corr(const float* __restrict__ raw, int nx, int ny, int ax, int ay, int W,
-                                              const float2* __restrict__ shifts, const float2* __restrict__ cs,
-                                              const float* __restrict__ local, int P, int fill,
-                                              float* __restrict__ aln, uint8_t* __restrict__ empty)
+// GCorrPatchShift.cu:61-104 (mGCorrect) with the local shift of :18-49: the
+// raw pixel that aligned pixel (X, Y) of frame t takes — its centred
+// coordinates rotated by the tilt axis, moved by the weighted patch shift and
+// the global shift, then int() of coordinate + 0.5 — as an index into the raw
+// frame, or -1 outside it.  The FP32 expressions are the reference's.
+// local: [5][P] of this tilt = patch centre x, centre y, shift x, shift y, good flag.
+__device__ __forceinline__ long long corr_src(int X, int Y, int nx, int ny, int ay, int W, float2 r, float2 sh,
+                                              const float* __restrict__ lp, int P)
 {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int X = blockIdx.x * 32 + (warp & 3) * 8 + (lane & 7);
-    const int Y = blockIdx.y * 8 + (warp >> 2) * 4 + (lane >> 3);
-    const int t = blockIdx.z;
-    if (X >= ax || Y >= ay) return;
-    float* o = aln + ((size_t)t * ay + Y) * ax;
-    if (X >= W) {
-        o[X] = 0.f;
-        return;
-    }
     float fx = X + 0.5f - W * 0.5f;
     float fy = Y + 0.5f - ay * 0.5f;
-    const float2 r = cs[t];
     const float ft = fx * r.x - fy * r.y;
     fy = fx * r.y + fy * r.x;
     fx = ft;
-    if (P > 0 && local) {
-        const float* lp = local + (size_t)t * 5 * P;
+    if (P > 0 && lp) {
         int cnt = 0;
         float sx = 0.f, sy = 0.f, sw = 0.f;
         for (int p = 0; p < P; p++) {
@@ -100,43 +81,107 @@ __global__ void __launch_bounds__(256) k_corr(const float* __restrict__ raw, int
         fx += dx;
         fy += dy;
     }
-    const float2 sh = shifts[t];
     fx += (sh.x + nx * 0.5f);
     fy += (sh.y + ny * 0.5f);
     const int x = (int)(fx + 0.5f), y = (int)(fy + 0.5f);
-    float v = -1e30f;
-    if (x >= 0 && x < nx && y >= 0 && y < ny) v = __ldg(raw + ((size_t)t * ny + y) * nx + x);
-    o[X] = v;
-    if (fill) empty[(size_t)t * W * ay + (size_t)Y * W + X] = v < -1e10f ? 1 : 0;
+    return (x >= 0 && x < nx && y >= 0 && y < ny) ? (long long)y * nx + x : -1;
+}
+
+// The aligned frames: pixel (X, Y) = the raw pixel corr_src picks, -1e30
+// outside the raw frame; columns X >= W (the odd-width case) are 0.  With
+// `fill`, the empty mask of the fill is written alongside.
+// A CTA covers a 32 x 32 tile; each warp an 8 x 4 patch, four times (rows
+// 8 apart), so the raw pixels a warp gathers lie within a few rows and
+// columns whatever the rotation (a 32 x 1 warp on a frame rotated by ~90
+// degrees would read 32 raw rows), and every thread has four independent
+// gathers in flight.  Tiles are visited along x (grid (ceil(ax / 32),
+// ceil(ay / 32), T)), or with `by_rows` along y (grid (ceil(ay / 32),
+// ceil(ax / 32), T)): for an axis near 90 degrees aligned y runs along raw
+// rows, so consecutive CTAs then read neighbouring pieces of the same raw
+// rows.  256 threads.
+__global__ void __launch_bounds__(256) k_corr(const float* __restrict__ raw, int nx, int ny, int ax, int ay, int W,
+                                              const float2* __restrict__ shifts, const float2* __restrict__ cs,
+                                              const float* __restrict__ local, int P, int fill, int by_rows,
+                                              float* __restrict__ aln, uint8_t* __restrict__ empty)
+{
+    constexpr int K = 4;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int tx = by_rows ? blockIdx.y : blockIdx.x, ty = by_rows ? blockIdx.x : blockIdx.y;
+    const int X = tx * 32 + (warp & 3) * 8 + (lane & 7);
+    const int Y0 = ty * 32 + (warp >> 2) * 4 + (lane >> 3);
+    const int t = blockIdx.z;
+    if (X >= ax) return;
+    const float2 r = cs[t], sh = shifts[t];
+    const float* lp = local ? local + (size_t)t * 5 * P : nullptr;
+    const float* rt = raw + (size_t)t * ny * nx;
+    long long src[K];
+#pragma unroll
+    for (int k = 0; k < K; k++) {
+        const int Y = Y0 + 8 * k;
+        src[k] = (Y < ay && X < W) ? corr_src(X, Y, nx, ny, ay, W, r, sh, lp, P) : -1;
+    }
+    float v[K];
+#pragma unroll
+    for (int k = 0; k < K; k++) v[k] = src[k] >= 0 ? __ldg(rt + src[k]) : -1e30f;
+#pragma unroll
+    for (int k = 0; k < K; k++) {
+        const int Y = Y0 + 8 * k;
+        if (Y >= ay) continue;
+        aln[((size_t)t * ay + Y) * ax + X] = X < W ? v[k] : 0.f;
+        if (fill && X < W) empty[(size_t)t * W * ay + (size_t)Y * W + X] = v[k] < -1e10f ? 1 : 0;
+    }
 }
 
 // GFillEmpty2D.cu:62-87: an empty pixel takes the value of the first
 // non-empty pixel along its chain r[i], r[r[i]], ... (at most 100 links).  A
 // pixel whose chain finds none keeps its value (below -1e10) and flags its
 // frame for k_fill_mean, which gives it the frame mean as the reference does.
-// Only empty pixels are written and only non-empty ones are read, so the
-// result does not depend on thread order.  Grid (ceil(W*ay / 256), T).
+// Only empty pixels are written and only non-empty ones are used, so the
+// result does not depend on thread order.  Each thread follows four chains
+// (pixels 256 apart) in step, and reads a link's flag and value together, so
+// that its random reads overlap.  Grid (ceil(W*ay / 1024), T), 256 threads.
 __global__ void __launch_bounds__(256) k_fill(float* __restrict__ aln, const uint8_t* __restrict__ empty,
                                               const int* __restrict__ r, int W, int ax, int ay,
                                               int* __restrict__ flags)
 {
-    const int n = W * ay;
-    const int i = blockIdx.x * blockDim.x + threadIdx.x, t = blockIdx.y;
-    if (i >= n) return;
+    constexpr int K = 4;
+    const int n = W * ay, t = blockIdx.y;
+    const int base = blockIdx.x * (256 * K) + threadIdx.x;
     const uint8_t* e = empty + (size_t)t * n;
-    if (!e[i]) return;
     float* f = aln + (size_t)t * ay * ax;
-    int next = __ldg(r + i);
-    for (int j = 0; j < 100; j++) {
-        if (e[next]) {
-            next = __ldg(r + next);
-            continue;
-        }
-        const int yn = next / W, yi = i / W;
-        f[(size_t)yi * ax + (i - yi * W)] = f[(size_t)yn * ax + (next - yn * W)];
-        return;
+    int cur[K];
+    bool act[K];
+#pragma unroll
+    for (int k = 0; k < K; k++) {
+        const int i = base + 256 * k;
+        act[k] = i < n && e[i];
+        cur[k] = act[k] ? __ldg(r + i) : 0;
     }
-    flags[t] = 1;
+    bool any = act[0] || act[1] || act[2] || act[3];
+    for (int j = 0; j < 100 && any; j++) {
+        any = false;
+        uint8_t ek[K];
+        float fv[K];
+#pragma unroll
+        for (int k = 0; k < K; k++) {
+            const int yn = cur[k] / W;
+            ek[k] = act[k] ? e[cur[k]] : 0;
+            fv[k] = act[k] ? f[(size_t)yn * ax + (cur[k] - yn * W)] : 0.f;
+        }
+#pragma unroll
+        for (int k = 0; k < K; k++) {
+            if (!act[k]) continue;
+            if (ek[k]) {
+                cur[k] = __ldg(r + cur[k]);
+                any = true;
+            } else {
+                const int i = base + 256 * k, yi = i / W;
+                f[(size_t)yi * ax + (i - yi * W)] = fv[k];
+                act[k] = false;
+            }
+        }
+    }
+    if (act[0] || act[1] || act[2] || act[3]) flags[t] = 1;
 }
 
 // GFillEmpty2D.cu:24-60 (mGCalcMean), for the frames k_fill flagged: the mean
