@@ -809,7 +809,9 @@ def run_stack_arm(args):
                                                "k_bin_cols, k_bin_c2r)",
                      "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                      "frac": achieved / peaks["hbm_gbs"], "peak_source": peaks["source"],
-                     "traffic": None, "bytes_per_step": bpt * T},
+                     "traffic": (profiled_traffic("all", "stack_4k", "f32") if c["name"] == "stack_4k" and T == 41
+                                 else None),
+                     "bytes_per_step": bpt * T},
         "clocks": clk,
     }
     st.close()
