@@ -817,7 +817,6 @@ def run_stack_arm(args):
     st.close()
     if not args.no_cpu_baseline:
         line["cpu_baseline"] = stack_cpu_baseline(c, frames)
-        line["reference_cuda"] = stack_reference_cuda(c, frames)
         line["error"] = stack_error(c, frames, dev_out, (ax, ay), (bx, by))
     print(json.dumps(line), flush=True)
 
@@ -842,36 +841,6 @@ def stack_cpu_baseline(c, frames, n=None):
     units = float(c["nx"]) * c["ny"] * n
     return {"value": units / dt / 1e9, "unit": STACK_UNIT, "cores": threads, "kind": "port",
             "sample": f"{n} of {len(c['tilts'])} tilts, FP64 C++ restatement, one tilt per thread, {dt:.2f} s"}
-
-
-def stack_reference_cuda(c, frames):
-    """The reference's own CUDA input stage (oracle/_ref/ref_stack, built from
-    its sources): GCorrPatchShift + the Fourier crop of CFourierCropImage per
-    tilt, with its per-tilt host copies, on the same series."""
-    exe = os.path.join(ROOT, "oracle", "_ref", "ref_stack")
-    if not os.path.exists(exe):
-        return None
-    T, ny, nx = frames.shape
-    d = "/dev/shm" if os.path.isdir("/dev/shm") else None
-    with tempfile.TemporaryDirectory(dir=d) as td:
-        fin, fpar, fout = (os.path.join(td, n) for n in ("in.bin", "par.bin", "out.bin"))
-        with open(fin, "wb") as f:
-            np.array([nx, ny, T], np.int32).tofile(f)
-            np.asarray(c["tilts"], np.float32).tofile(f)
-            frames.tofile(f)
-        with open(fpar, "wb") as f:
-            np.array([0, 0], np.int32).tofile(f)
-            c["shifts"].tofile(f)
-            c["axes"].tofile(f)
-        r = subprocess.run([exe, "stack", fin, fpar, fout, str(c["seed"]), repr(c["bin"]), repr(float(c["axes"][0])),
-                            "noaligned"], capture_output=True, text=True, timeout=600)
-        if r.returncode != 0:
-            return {"error": r.stderr[-300:]}
-        info = json.loads([ln for ln in r.stdout.splitlines() if ln.startswith("{")][-1])
-    sec = info["seconds"]
-    return {"value": float(nx) * ny * T / sec / 1e9, "unit": STACK_UNIT, "seconds": sec,
-            "what": "reference CUDA CCorrTomoStack path per tilt: pageable H2D, GCorrPatchShift + fill, "
-                    "2-D cuFFT crop, row-wise unpad to host"}
 
 
 def stack_error(c, frames, out, aligned_xy, binned_xy, n=2):
