@@ -50,27 +50,31 @@ __global__ void k_axis_cs(const float* __restrict__ rad, int T, float2* __restri
 // raw pixel that aligned pixel (X, Y) of frame t takes — its centred
 // coordinates rotated by the tilt axis, moved by the weighted patch shift and
 // the global shift, then int() of coordinate + 0.5 — as an index into the raw
-// frame, or -1 outside it.  The FP32 expressions are the reference's.
+// frame, or -1 outside it.  The FP32 operations are the ones the reference's
+// kernel executes, written out: nvcc contracts its rotation
+// x*c - y*s, x*s + y*c into fma(x, c, -(y*s)), fma(y, c, x*s) (established
+// on 4096^2 frames, where the other contractions pick a different raw pixel
+// for about one pixel in 10^5).
 // local: [5][P] of this tilt = patch centre x, centre y, shift x, shift y, good flag.
 __device__ __forceinline__ long long corr_src(int X, int Y, int nx, int ny, int ay, int W, float2 r, float2 sh,
                                               const float* __restrict__ lp, int P)
 {
     float fx = X + 0.5f - W * 0.5f;
     float fy = Y + 0.5f - ay * 0.5f;
-    const float ft = fx * r.x - fy * r.y;
-    fy = fx * r.y + fy * r.x;
+    const float ft = __fmaf_rn(fx, r.x, -__fmul_rn(fy, r.y));
+    fy = __fmaf_rn(fy, r.x, __fmul_rn(fx, r.y));
     fx = ft;
     if (P > 0 && lp) {
         int cnt = 0;
         float sx = 0.f, sy = 0.f, sw = 0.f;
         for (int p = 0; p < P; p++) {
             if (__ldg(lp + 4 * P + p) < 0.9f) continue;
-            const float lx = (fx - __ldg(lp + p)) / nx;
-            const float ly = (fy - __ldg(lp + P + p)) / ny;
-            const float w = expf(-100.0f * (lx * lx + ly * ly));
-            sx += __ldg(lp + 2 * P + p) * w;
-            sy += __ldg(lp + 3 * P + p) * w;
-            sw += w;
+            const float lx = __fdiv_rn(__fsub_rn(fx, __ldg(lp + p)), (float)nx);
+            const float ly = __fdiv_rn(__fsub_rn(fy, __ldg(lp + P + p)), (float)ny);
+            const float w = expf(__fmul_rn(-100.0f, __fmaf_rn(ly, ly, __fmul_rn(lx, lx))));
+            sx = __fmaf_rn(__ldg(lp + 2 * P + p), w, sx);
+            sy = __fmaf_rn(__ldg(lp + 3 * P + p), w, sy);
+            sw = __fadd_rn(sw, w);
             cnt += 1;
         }
         float dx = 0.f, dy = 0.f;

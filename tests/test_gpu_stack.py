@@ -62,6 +62,34 @@ def _mode(st):
     return 1 if st.c2r == recon.C2R_PACKED else 0
 
 
+def test_aligned_frames_equal_live_reference_at_4k():
+    # at 4096^2 the coordinates are large enough that a different rounding of
+    # the rotation picks another raw pixel for ~1 pixel in 10^5: every aligned
+    # pixel (fill included) must be the reference kernel's
+    import os
+    if not os.path.exists(os.path.join(ol.ROOT, "oracle", "_ref", "ref_stack")):
+        pytest.skip("oracle/_ref/ref_stack not built")
+    import sys
+    sys.path.insert(0, os.path.join(ol.ROOT, "tests", "golden"))
+    import gen_golden
+    rng = np.random.default_rng(3)
+    T = 2
+    frames = synth.make_tilt_series(4096, 4096, synth.tilt_range(-3, 3, 6), 300,
+                                    synth.Phantom(seed=9, n_ellipsoids=150, axis_min=20.0, axis_max=160.0, n_beads=10))
+    c = dict(shifts=rng.uniform(-20, 20, (T, 2)).astype(np.float32),
+             axes=rng.uniform(85.0, 87.0, T).astype(np.float32), shift_only=0, bin=1.0, local=None, seed=4242)
+    c["size_axis"] = float(c["axes"][0])
+    al_ref, _, table_ref, _ = gen_golden.run_reference_stack(frames, synth.tilt_range(-3, 3, 6), c)
+    st = recon.Stack(4096, 4096, T, shifts=c["shifts"], tilt_axes=c["axes"], size_axis=c["size_axis"], seed=4242,
+                     bin=1.0)
+    try:
+        assert np.array_equal(st.fill_table(), table_ref)
+        out = st.run_host([f for f in frames])
+    finally:
+        st.close()
+    assert np.array_equal(out, al_ref)
+
+
 def test_device_path_equals_host_path():
     import torch
     rng = np.random.default_rng(5)
