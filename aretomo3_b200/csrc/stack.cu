@@ -627,29 +627,39 @@ at3r_status at3r_stack_create(const at3r_stack_geom* g, at3r_stack** out)
         float* d_rad = nullptr;
         if ((rc = salloc(&s->d_shift, T)) || (rc = salloc(&s->d_cs, T)) || (rc = salloc(&d_rad, T)))
             return fail(rc);
-        if (cudaMemcpy(s->d_shift, sh.data(), sizeof(float2) * T, cudaMemcpyHostToDevice) != cudaSuccess ||
-            cudaMemcpy(d_rad, rad.data(), sizeof(float) * T, cudaMemcpyHostToDevice) != cudaSuccess) {
-            cudaFree(d_rad);
-            return fail(st_err(AT3R_ERR_CUDA, "alignment upload failed"));
+        // set-up kernels on a private stream, so that other work on the device is not waited for
+        cudaStream_t ss = nullptr;
+        cudaError_t e = cudaStreamCreateWithFlags(&ss, cudaStreamNonBlocking);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(s->d_shift, sh.data(), sizeof(float2) * T, cudaMemcpyHostToDevice, ss);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(d_rad, rad.data(), sizeof(float) * T, cudaMemcpyHostToDevice, ss);
+        if (e == cudaSuccess) {
+            k_axis_cs<<<(s->T + 127) / 128, 128, 0, ss>>>(d_rad, s->T, s->d_cs);
+            e = cudaGetLastError();
         }
-        k_axis_cs<<<(s->T + 127) / 128, 128>>>(d_rad, s->T, s->d_cs);
-        const cudaError_t e = cudaDeviceSynchronize();
+        if (e == cudaSuccess && g->rand_fill) {
+            // one table per set-up, as GFillEmpty2D::SetSize draws it (GFillEmpty2D.cu:100-116)
+            const int npx = s->W * s->ay;
+            if ((rc = salloc(&s->d_rand, (size_t)npx))) {
+                cudaStreamSynchronize(ss);
+                cudaStreamDestroy(ss);
+                cudaFree(d_rad);
+                return fail(rc);
+            }
+            k_rand_table<<<(npx + 255) / 256, 256, 0, ss>>>(s->d_rand, npx, g->seed);
+            e = cudaGetLastError();
+        }
+        if (e == cudaSuccess) e = cudaStreamSynchronize(ss);
+        if (ss) cudaStreamDestroy(ss);
         cudaFree(d_rad);
-        if (e != cudaSuccess) return fail(st_err(AT3R_ERR_CUDA, std::string("rotation table: ") + cudaGetErrorString(e)));
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            return fail(st_err(AT3R_ERR_CUDA, std::string("alignment tables: ") + cudaGetErrorString(e)));
+        }
         if (s->P > 0) {
             if ((rc = salloc(&s->d_local, T * 5 * s->P))) return fail(rc);
             if (cudaMemcpy(s->d_local, g->local_params, sizeof(float) * T * 5 * s->P, cudaMemcpyHostToDevice) !=
                 cudaSuccess)
                 return fail(st_err(AT3R_ERR_CUDA, "local alignment upload failed"));
-        }
-        if (g->rand_fill) {
-            // one table per set-up, as GFillEmpty2D::SetSize draws it (GFillEmpty2D.cu:100-116)
-            const int npx = s->W * s->ay;
-            if ((rc = salloc(&s->d_rand, (size_t)npx))) return fail(rc);
-            k_rand_table<<<(npx + 255) / 256, 256>>>(s->d_rand, npx, g->seed);
-            const cudaError_t e2 = cudaDeviceSynchronize();
-            if (e2 != cudaSuccess)
-                return fail(st_err(AT3R_ERR_CUDA, std::string("random table: ") + cudaGetErrorString(e2)));
         }
     }
 

@@ -89,3 +89,44 @@ def test_reproj_range_matches_oracle_without_gpu():
         skip = (rng.random(T) < 0.15).astype(np.uint8)
         skip[p] = 1
         assert recon.reproj_range(tilts, p, skip) == ol.reproj_range(tilts, p, skip)
+
+
+@pytest.mark.parametrize("kw", [
+    dict(nx=1),                                   # too narrow
+    dict(bin=0.5),                                # binning below 1
+    dict(local_params=None, num_patches=3),       # patches without parameters
+])
+def test_invalid_stack_geometry_is_rejected_without_gpu(kw):
+    from aretomo3_b200 import recon
+    g, keep = recon._stack_geom(64, 48, 3, seed=0)
+    for k, v in kw.items():
+        setattr(g, k, v if not isinstance(v, float) else float(v))
+    h = ctypes.c_void_p()
+    rc = recon.lib().at3r_stack_create(ctypes.byref(g), ctypes.byref(h))
+    assert rc == 1 and not h.value   # AT3R_ERR_INVALID_ARGUMENT, nothing created
+
+
+def test_invalid_thickness_arguments_are_rejected_without_gpu():
+    from aretomo3_b200 import recon
+    g, keep = recon._stack_geom(64, 48, 3, seed=0)
+    tilts = np.zeros(3, np.float32)
+    frames = [np.zeros((48, 64), np.float32) for _ in range(3)]
+    P = ctypes.c_void_p * 3
+    r = recon.ThicknessResult()
+    L = recon.lib()
+    # pixel size 0
+    assert L.at3r_thickness_host(ctypes.byref(g), tilts.ctypes.data, 0.0, P(*[f.ctypes.data for f in frames]),
+                                 None, None, 0, ctypes.byref(r), None) == 1
+    # a missing frame
+    assert L.at3r_thickness_host(ctypes.byref(g), tilts.ctypes.data, 1.0, P(frames[0].ctypes.data, None, None),
+                                 None, None, 0, ctypes.byref(r), None) == 1
+
+
+def test_stack_without_gpu_reports_no_device():
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    from aretomo3_b200 import recon
+    with pytest.raises(recon.ReconError) as ei:
+        recon.Stack(64, 48, 3, seed=0)
+    assert ei.value.status == 6  # AT3R_ERR_NO_DEVICE
