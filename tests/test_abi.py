@@ -130,3 +130,12 @@ def test_stack_without_gpu_reports_no_device():
     with pytest.raises(recon.ReconError) as ei:
         recon.Stack(64, 48, 3, seed=0)
     assert ei.value.status == 6  # AT3R_ERR_NO_DEVICE
+
+
+def test_corr_tomo_stack_mirror_refuses_paths_that_are_not_built():
+    from aretomo3_b200 import recon
+    c = recon.CCorrTomoStack()
+    with pytest.raises(NotImplementedError):
+        c.Set2(2.0, False, True)       # real-space binning (GBinImage2D)
+    with pytest.raises(NotImplementedError):
+        c.Set3(False, False, True)     # R-weighted corrected stack
