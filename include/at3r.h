@@ -19,10 +19,10 @@
  *                         CDoWbpRecon::DoIt / CDoSartRecon::DoIt return
  *   volume, host        : ny frame pointers, each float[Nz][Nx]
  *
- * Errors are returned as status codes; nothing aborts the process.  A plan is
- * not safe to run from two host threads at once; distinct plans are
- * independent (no module-global device state).  `stream` is a cudaStream_t
- * (NULL = the legacy default stream).
+ * Errors are returned as status codes; nothing aborts the process.  A plan (or
+ * a stack, below) is not safe to run from two host threads at once; distinct
+ * plans and stacks are independent (no module-global device state).  `stream`
+ * is a cudaStream_t (NULL = the legacy default stream).
  */
 #ifndef AT3R_H
 #define AT3R_H
