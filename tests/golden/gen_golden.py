@@ -3,7 +3,7 @@ own CUDA Recon (AreTomo3 AreTomo/Recon, compiled for sm_100a from the
 reference sources by oracle/ref/build_ref.sh into oracle/_ref/ref_recon) on
 seeded synthetic tilt series.  It needs a GPU, so it runs on a B200 box:
 
-    python tests/golden/gen_golden.py --out gpurun_out/golden
+    python tests/golden/gen_golden.py --out <dir>
 
 and the resulting ``*.npz`` files are committed here.  Each fixture holds the
 input frames, the tilt angles, the reconstruction parameters and the volume

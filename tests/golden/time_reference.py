@@ -3,7 +3,7 @@ reference sources for sm_100a) against this implementation's host-path entry
 points on the same seeded series, on one GPU.  Test infrastructure: it runs
 on a B200 box,
 
-    python tests/golden/time_reference.py [--only recon,reproj,stack,thick] > gpurun_out/reference_timing.json
+    python tests/golden/time_reference.py [--only recon,reproj,stack,thick] > reference_timing.json
 
 and prints one JSON line per workload: the reference's DoIt wall time (host
 frames in, host XZ frames out, its own timer around DoIt), ours through
