@@ -132,3 +132,22 @@ def test_thickness_edges_known_answer():
     lo, hi, thick, off = res
     assert 20 * 20 <= lo <= 32 * 20 and 66 * 20 <= hi <= 80 * 20
     assert thick == hi - lo and off == (lo + hi) // 2 - int(50 * 20.0)
+
+
+def test_odd_width_covers_one_column_less():
+    # GCorrPatchShift / GFillEmpty2D cover (padX/2 - 1) * 2 columns: ax - 1 for an odd ax;
+    # the last column is 0 here (the reference leaves it unwritten)
+    rng = np.random.default_rng(4)
+    raw = rng.standard_normal((2, 14, 17)).astype(np.float32)
+    table = rng.integers(0, 16 * 14, size=16 * 14).astype(np.int32)
+    _, al = ol.stack(raw, shifts=np.zeros((2, 2), np.float32), table=table)
+    assert al.shape == (2, 14, 17)
+    assert np.all(al[:, :, 16] == 0.0)
+    assert np.all(al[:, :, :16] > -1e10)     # every covered pixel filled
+
+
+def test_bin_only_equal_sizes_is_a_copy():
+    rng = np.random.default_rng(5)
+    raw = rng.standard_normal((2, 20, 30)).astype(np.float32)
+    out, _ = ol.stack(raw, correct=False, rand_fill=False, bin=1.0)
+    assert np.array_equal(out.astype(np.float32), raw)
