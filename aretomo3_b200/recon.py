@@ -735,3 +735,42 @@ class CCalcVolThick:
 
     def GetHighEdge(self, angstrom: bool = False) -> float:
         return float(np.float32(self.m_aiSampleEdges[1]) * (self.m_fPixSize if angstrom else np.float32(1)))
+
+
+def recon_series(tilt_series: "TiltSeries", align_param: "AlignParam", vol_z: int, at_bin: float = 1.0,
+                 method: int = WBP, local_param: "LocalAlignParam | None" = None, seed=None, start_tilt: int = 0,
+                 num_tilts: int | None = None, iterations: int = 0, subsets: int = 1, **plan_kw) -> np.ndarray:
+    """The reconstruction step of CAreTomoMain::mRecon / mReconVol
+    (AreTomo/CAreTomoMain.cpp:727-761, 809-879) on one GPU: the aligned series
+    (CCorrTomoStack with Fourier cropping, rotation by the tilt axes, local
+    patches if given), Fourier-binned by at_bin (CBinStack::DoFFT), then WBP or
+    SART of thickness vol_z (of the binned series).  The binned series stays on
+    the device between the two stages; the volume [by][vol_z][bx & ~1] comes
+    back to host memory.  seed: the fill's random table (None: the time, as
+    the reference)."""
+    import torch
+    nx, ny, nt = tilt_series.stk_size
+    axes = np.asarray([align_param.GetTiltAxis(i) for i in range(nt)], np.float32)
+    st = Stack(nx, ny, nt, shifts=np.asarray([align_param.GetShift(i) for i in range(nt)], np.float32),
+               tilt_axes=axes, size_axis=float(axes[0]),
+               local_params=None if local_param is None else local_param.params, rand_fill=True, seed=seed,
+               bin=at_bin)
+    try:
+        dev = torch.device("cuda", torch.cuda.current_device())
+        stream = torch.cuda.current_stream(dev)
+        raw = torch.from_numpy(np.ascontiguousarray(tilt_series.frames, np.float32)).to(dev)
+        binned = torch.empty(st.binned_shape, device=dev, dtype=torch.float32)
+        st.run_device(raw.data_ptr(), binned.data_ptr(), stream.cuda_stream)
+        del raw
+    finally:
+        st.close()
+    kw = dict(plan_kw)
+    if method == SART:
+        kw.update(start_tilt=start_tilt, num_tilts=nt if num_tilts is None else num_tilts, iterations=iterations,
+                  subsets=subsets)
+    vol, plan = reconstruct_device(binned, align_param.GetTilts(False)[:nt], vol_z, method=method, stream=stream, **kw)
+    try:
+        out = vol.cpu().numpy()
+    finally:
+        plan.close()
+    return out

@@ -249,3 +249,29 @@ def test_thickness_post_processing_equals_oracle_on_the_same_volume():
     sm, res = ol.thickness_edges(c.profile, r.binning)
     assert np.array_equal(sm, c.profile_smoothed)
     assert list(res) == [r.edges[0], r.edges[1], r.thickness, r.offset_z]
+
+
+@pytest.mark.parametrize("method", [recon.WBP, recon.SART])
+def test_recon_series_keeps_the_binned_series_on_the_device(method):
+    # CAreTomoMain::mRecon's data flow (aligned, binned, reconstructed) with the
+    # binned series kept on the device equals the two host-path stages
+    rng = np.random.default_rng(21)
+    T, ny, nx = 11, 256, 320
+    tilts = synth.tilt_range(-60, 60, 12)
+    frames = synth.make_tilt_series(nx, ny, tilts, 80, synth.Phantom(seed=6, n_ellipsoids=60, n_beads=6))
+    ap = recon.AlignParam(tilts=tilts, shifts=rng.uniform(-6, 6, (T, 2)).astype(np.float32),
+                          tilt_axes=rng.uniform(-2, 2, T).astype(np.float32))
+    kw = dict(iterations=3, subsets=4) if method == recon.SART else {}
+    got = recon.recon_series(recon.TiltSeries(frames), ap, 48, at_bin=2.0, method=method, seed=5, **kw)
+    st = recon.Stack(nx, ny, T, shifts=ap.shifts, tilt_axes=ap.tilt_axes, size_axis=float(ap.tilt_axes[0]), seed=5,
+                     bin=2.0)
+    try:
+        binned = st.run_host([f for f in frames])
+    finally:
+        st.close()
+    if method == recon.WBP:
+        ref = recon.CDoWbpRecon().DoIt(recon.TiltSeries(binned), ap, 48)
+    else:
+        ref = recon.CDoSartRecon().DoIt(recon.TiltSeries(binned), ap, 0, T, 48, 3, 4)
+    assert got.shape == ref.shape
+    assert np.array_equal(got, ref)
