@@ -38,7 +38,7 @@ def build_at3r(force: bool = False) -> str:
     srcs.append(os.path.join(ROOT, "include", "at3r.h"))
     if not (force or _newer(out, srcs)):
         return out
-    units = ["at3r.cu", "reproj.cu", "stack.cu", "at3r_server.cpp"]
+    units = ["at3r.cu", "reproj.cu", "stack.cu", "at3r_server.cpp", "mrc.cpp"]
     bdir = os.path.join(CSRC, "_build")
     os.makedirs(bdir, exist_ok=True)
     common = [NVCC, *ARCH, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-I", os.path.join(ROOT, "include")]

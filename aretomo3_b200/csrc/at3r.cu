@@ -1197,6 +1197,7 @@ const char* at3r_status_str(at3r_status s)
         case AT3R_ERR_UNSUPPORTED: return "unsupported option";
         case AT3R_ERR_TOO_LARGE: return "size exceeds a kernel limit";
         case AT3R_ERR_NO_DEVICE: return "no CUDA device";
+        case AT3R_ERR_IO: return "file error";
     }
     return "unknown status";
 }

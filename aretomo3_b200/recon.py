@@ -14,6 +14,7 @@ All computation runs in libat3r.so on the GPU; there is no CPU path.
 from __future__ import annotations
 
 import ctypes
+import os
 import time
 from dataclasses import dataclass, field
 
@@ -122,6 +123,8 @@ _EXPORTS = {
     "at3r_thickness_host": (ctypes.c_int, [ctypes.POINTER(StackGeom), ctypes.c_void_p, ctypes.c_float,
                                            ctypes.POINTER(ctypes.c_void_p), ctypes.c_void_p, ctypes.c_void_p,
                                            ctypes.c_int, ctypes.POINTER(ThicknessResult), ctypes.c_void_p]),
+    "at3r_mrc_write": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(ctypes.c_void_p), ctypes.c_int, ctypes.c_int,
+                                      ctypes.c_int, ctypes.c_float]),
     "at3r_status_str": (ctypes.c_char_p, [ctypes.c_int]),
     "at3r_last_error": (ctypes.c_char_p, []),
 }
@@ -774,3 +777,16 @@ def recon_series(tilt_series: "TiltSeries", align_param: "AlignParam", vol_z: in
     finally:
         plan.close()
     return out
+
+
+def save_mrc(path: str, frames, pix_size: float = 1.0) -> None:
+    """The volume file CAsyncSaveVol::mSaveVol writes (DataUtil/
+    CAsyncSaveVol.cpp:82-126): frames [nz][ny][nx] (an array, or a list of
+    equal-sized 2-D frames) as a float MRC with the reference writer's header."""
+    fr = [np.ascontiguousarray(f, np.float32) for f in frames]
+    if not fr or any(f.ndim != 2 or f.shape != fr[0].shape for f in fr):
+        raise ValueError("frames must be equal-sized 2-D arrays")
+    ny, nx = fr[0].shape
+    P = ctypes.c_void_p * len(fr)
+    _check(lib().at3r_mrc_write(os.fsencode(path), P(*[f.ctypes.data for f in fr]), nx, ny, len(fr),
+                                float(pix_size)))

@@ -41,7 +41,8 @@ typedef enum at3r_status {
     AT3R_ERR_OUT_OF_MEMORY = 3,
     AT3R_ERR_UNSUPPORTED = 4,
     AT3R_ERR_TOO_LARGE = 5,
-    AT3R_ERR_NO_DEVICE = 6
+    AT3R_ERR_NO_DEVICE = 6,
+    AT3R_ERR_IO = 7
 } at3r_status;
 
 typedef enum at3r_method { AT3R_WBP = 0, AT3R_SART = 1 } at3r_method;
@@ -321,6 +322,20 @@ at3r_status at3r_thickness_device(const at3r_stack_geom* g, const float* tilts_d
 at3r_status at3r_thickness_host(const at3r_stack_geom* g, const float* tilts_deg, float pix_size,
                                 const float* const* frames, float* profile, float* profile_smoothed,
                                 int profile_cap, at3r_thickness* result, void* stream);
+
+/* ---- Volume file: the MRC file CAsyncSaveVol::mSaveVol writes -------------
+ * (DataUtil/CAsyncSaveVol.cpp:82-126 through LibSrc/Mrcfile CSaveMrc): the
+ * 1024-byte main header — nx, ny, nz, mode 2 (float), sampling equal to the
+ * size, cell = size x pix_size, angles 90, axes 1 2 3, min / max / mean 0,
+ * and the writer's defaults (extended-header type "AGAR", version 20140,
+ * dvid -16224, sub 1, type 5, tilt angles 90, "MAP" and the machine stamp) —
+ * with no extended header (CSaveMrc::SetImgSize resets the one asked for
+ * before it), then the nz frames of nx x ny floats.  frames: nz host
+ * pointers, e.g. the XY frames of at3r_run_host_xyz (nx = Nx, ny = ny, nz =
+ * Nz) or the XZ frames of at3r_run_host (nx = Nx, ny = Nz, nz = ny).
+ * Frames are written by up to four threads at their offsets.
+ * AT3R_ERR_IO when the file cannot be written. */
+at3r_status at3r_mrc_write(const char* path, const float* const* frames, int nx, int ny, int nz, float pix_size);
 
 const char* at3r_status_str(at3r_status s);
 const char* at3r_last_error(void);

@@ -6,7 +6,9 @@
 # re-projector (AreTomo/ProjAlign/GReproj + CCalcReproj) into
 # oracle/_ref/ref_reproj; and its input stage (AreTomo/Correct/GCorrPatchShift
 # + the Fourier crop of CFourierCropImage) with the thickness measurement
-# (AreTomo/Recon/CCalcVolThick) into oracle/_ref/ref_stack.  Nothing is copied out of the
+# (AreTomo/Recon/CCalcVolThick) into oracle/_ref/ref_stack; and its MRC volume
+# writer (LibSrc/Mrcfile CSaveMrc, host C++ only) into oracle/_ref/ref_mrc.
+# Nothing is copied out of the
 # reference tree; objects go to oracle/_ref/obj.
 set -euo pipefail
 REF=${AT3R_REFERENCE:-/root/reference}
@@ -76,3 +78,16 @@ g++ $CXXFLAGS -c "$HERE/ref_stack_driver.cpp" -o "$OBJ/ref_stack_driver.o"
 $NVCC -gencode arch=compute_100a,code=sm_100a -o "$OUT/ref_stack" "${objs[@]}" "${st[@]}" \
   "$OBJ/ref_stub.o" "$OBJ/ref_stack_stub.o" "$OBJ/ref_stack_driver.o" -lcufft -lcurand -lcuda
 echo "built $OUT/ref_stack"
+
+# the MRC volume writer (LibSrc/Mrcfile, host code: builds and runs without a GPU)
+mr=()
+for f in LibSrc/Mrcfile/App/CSaveMrc LibSrc/Mrcfile/Header/CSaveMainHeader LibSrc/Mrcfile/Header/CSaveExtHeader \
+         LibSrc/Mrcfile/Header/CMainHeader LibSrc/Mrcfile/Image/CSaveImage LibSrc/Util/Util_FileName \
+         LibSrc/Util/Util_SwapByte LibSrc/Util/Util_String; do
+  o="$OBJ/$(echo "$f" | tr / _).o"
+  [ "$o" -nt "$REF/$f.cpp" ] || g++ $CXXFLAGS -w -I"$REF/LibSrc" -c "$REF/$f.cpp" -o "$o"
+  mr+=("$o")
+done
+g++ $CXXFLAGS -I"$REF/LibSrc" -c "$HERE/ref_mrc_driver.cpp" -o "$OBJ/ref_mrc_driver.o"
+g++ -o "$OUT/ref_mrc" "${mr[@]}" "$OBJ/ref_mrc_driver.o"
+echo "built $OUT/ref_mrc"
