@@ -696,6 +696,16 @@ class CBinStack:
             st.close()
 
 
+def thickness_pixel_size(pix_size: float, nx: int, ny: int, tilt_axis: float, binned_y: int, binning) -> np.float32:
+    """The pixel size CCalcVolThick's edges are scaled by in Angstrom: the raw
+    pixel size times CCorrTomoStack's y binning (aligned y / binned y, the
+    aligned size as CCorrectUtil::CalcAlignedSize gives it), over the
+    binning (CCorrTomoStack.cpp:129-131, 180; CCalcVolThick.cpp:73)."""
+    aligned_y = nx if abs(np.sin(float(tilt_axis) * 3.14 / 180.0)) > 0.707 else ny
+    bin_y = np.float32(aligned_y) / np.float32(binned_y)
+    return np.float32(np.float32(np.float32(pix_size) * bin_y) / np.float32(binning))
+
+
 class CCalcVolThick:
     """Mirror of MAR::CCalcVolThick (AreTomo/Recon/CCalcVolThick.cpp:47-110):
     DoIt(series, alignment, pixel size) aligns and bins the series by
@@ -723,10 +733,7 @@ class CCalcVolThick:
         self.profile, self.profile_smoothed = prof[:n].copy(), prof_s[:n].copy()
         self.m_aiSampleEdges = (r.edges[0], r.edges[1])
         self.m_fBinning = np.float32(r.binning)
-        # pixel size of the binned series, CCorrTomoStack::DoIt and CCalcVolThick.cpp:73
-        a = (ny, nx) if abs(np.sin(float(axes[0]) * 3.14 / 180.0)) > 0.707 else (nx, ny)
-        bin_y = np.float32(a[1]) / np.float32(r.binned_xy[1])
-        self.m_fPixSize = np.float32(np.float32(np.float32(pix_size) * bin_y) / self.m_fBinning)
+        self.m_fPixSize = thickness_pixel_size(pix_size, nx, ny, float(axes[0]), r.binned_xy[1], self.m_fBinning)
         return self
 
     def GetThickness(self, angstrom: bool = False) -> float:

@@ -139,3 +139,13 @@ def test_corr_tomo_stack_mirror_refuses_paths_that_are_not_built():
         c.Set2(2.0, False, True)       # real-space binning (GBinImage2D)
     with pytest.raises(NotImplementedError):
         c.Set3(False, False, True)     # R-weighted corrected stack
+
+
+def test_thickness_pixel_size_follows_the_reference_arithmetic():
+    from aretomo3_b200 import recon
+    # 4096 x 4096 at 1 A, binning 20 -> 204 x 204: (1 * 4096/204) / 20
+    assert recon.thickness_pixel_size(1.0, 4096, 4096, 1.5, 204, 20.0) == np.float32(
+        np.float32(np.float32(4096) / np.float32(204)) / np.float32(20))
+    # an axis near 90 degrees sizes y by the raw x
+    assert recon.thickness_pixel_size(0.8, 5760, 4092, 86.0, 286, 25.0) == np.float32(
+        np.float32(np.float32(0.8) * (np.float32(5760) / np.float32(286))) / np.float32(25))
