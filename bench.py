@@ -1,10 +1,15 @@
 #!/usr/bin/env python
 """Benchmark of the reconstruction path on B200.
 
-Default workload (one GPU): SART on the seeded 1024 x 1024 x 61-tilt series
-(-60..60 step 2, thickness 300, 500 ellipsoids + 40 beads, Poisson noise at
-50 e-/px), 15 iterations, 5 subsets, relaxation 0.3.  A "step" is one full
-reconstruction of that series.
+Default workload (one GPU), `recon_4k`: the seeded 4096 x 4096 x 41-tilt
+series (-60..60 step 3, thickness 1200, 500 ellipsoids + 40 beads scaled to
+4k, Poisson noise at 50 e-/px).  The line's value is SART on it (15
+iterations, 5 subsets, relaxation 1/subsets, FP32); a "step" is one full
+reconstruction of the series.  Sub-records on the same frames: `wbp` (the
+metric's WBP half, FP32), `precision` (FP16 and BF16 storage of WBP and SART
+beside FP32, with their error against the FP64 oracle) and `reference_cuda`
+(the reference's own CUDA Recon, built from its sources, against this
+library's reference-shaped entry points on a band of rows).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload NAME]
 
@@ -12,21 +17,25 @@ Metric: GVoxel*tilt/s = Nx * ny * Nz * T of the output grid per second (the
 same count for WBP and SART; SART's iterations are work inside a step).
 
 * value    : device-resident (projections already in HBM), CUDA events on the
-             launching stream, max over ranks.  Inputs (256 MB of projections,
-             1.26 GB of volume) exceed the 126 MB L2.
+             launching stream, max over ranks.  Inputs (2.75 GB of projections,
+             80.5 GB of volume) exceed the 126 MB L2.
 * e2e      : the same through the host API (at3r_run_host): pinned host
-             frames in, host volume frames out, copies inside the timed region.
+             frames in, host volume frames out, copies inside the timed region
+             (--e2e-steps of them).
 * roofline : the kernel with the largest device time, its algorithmic bytes
              per launch / its mean launch time (CUDA events around every
-             launch on its stream, during a timed step), against the measured
-             HBM copy bandwidth.
-* cpu_baseline : the FP32 C++ port of the same math (oracle/, OpenMP over
-             y-slices) on the host cores, on a sample of the series' slices.
+             launch on its stream, during one instrumented step), against the
+             measured HBM copy bandwidth; plus its on-chip (L1/shared) figure.
+* cpu_baseline : the FP32 C++ port of the same math (oracle/, OpenMP) on the
+             host cores, on a sample of the series' slices.
+* error    : the volume's two middle slices against the FP64 oracle.
 
 With --impl reference the same workload is timed on the host cores by the
 FP32 port, rank 0 only (the reference's Recon has no CPU implementation).
 N > 1: torchrun, one process per GPU, each rank reconstructs its own series
-(weak scaling, no collective on the data path).
+(weak scaling, no collective on the data path); the sub-records are N = 1 only.
+Other workloads: --workload sart_1k | wbp_512 | wbp_4k | sart_4k | batch_uneven |
+serve_mix | stack_4k | thick_4k (and profiling cases, see workload()).
 """
 from __future__ import annotations
 
@@ -80,6 +89,15 @@ def workload(name: str, seed_offset: int = 0) -> dict:
     elif name == "sart_4k":
         c = synth.precision_4k(seed=3 + seed_offset)
         c.update(method="sart", relax=0.0, label="SART 4096x4096x41 tilts, thickness 1200, 15 iterations, 5 subsets")
+    elif name == "recon_4k":
+        # the 4096 x 4096 x 41 series both halves of the metric are quoted on:
+        # SART is the line's value, WBP / the 16-bit forms / the reference's own
+        # CUDA Recon are sub-records on the same frames
+        c = synth.precision_4k(seed=3 + seed_offset)
+        c.update(method="sart", relax=0.0, with_wbp=True, with_precision=True, with_reference_cuda=True,
+                 label="SART 4096x4096x41 tilts (-60..60 step 3), thickness 1200, 15 iterations, 5 subsets, "
+                       "relaxation 1/subsets; 500 ellipsoids + 40 beads, Poisson 50 e-/px",
+                 wbp_label="WBP 4096x4096x41 tilts (-60..60 step 3), thickness 1200, same frames")
     else:
         raise SystemExit(f"unknown workload {name}")
     c["name"] = name
@@ -255,7 +273,8 @@ def run_reference_arm(args, c, rank, world):
     from aretomo3_b200 import synth
     frames = synth.make_tilt_series(c["nx"], c["ny"], c["tilts"], c["vol_z"], c["phantom"])
     threads = os.cpu_count() or 1
-    s = min(max(4, cpu_sample_slices(c) // 3), c["ny"])
+    # a 4096-wide slice is seconds of work on all host threads: one per step
+    s = 1 if c["nx"] > 1024 else min(max(4, cpu_sample_slices(c) // 3), c["ny"])
     y0 = (c["ny"] - s) // 2
     for _ in range(args.warmup):
         cpu_port_run(c, frames, y0, min(y0 + 1, c["ny"]), threads)
@@ -276,136 +295,108 @@ def run_reference_arm(args, c, rank, world):
     print(json.dumps(line), flush=True)
 
 
-def run_our_arm(args, c, rank, world, local_rank):
+def _gpu_index(local_rank: int) -> int:
+    cvd = os.environ.get("CUDA_VISIBLE_DEVICES", "")
+    if cvd.replace(",", "").isdigit():
+        return int(cvd.split(",")[local_rank])
+    return local_rank
+
+
+def measure(c, frames, proj, vol, stream, steps, warmup, e2e_steps, world, gpu_index, instrument=True,
+            clocks=True):
+    """One plan over the series already in HBM: `warmup` untimed steps, then
+    `steps` timed ones (barrier + synchronize on both sides, CUDA events on the
+    launching stream, max over ranks), one instrumented step (an event pair
+    around every launch) for the per-kernel shares, and `e2e_steps` through the
+    host API (pinned frames in, pinned volume frames out, copies inside the
+    timed region).  Returns a dict of the measurements; the volume's two middle
+    slices are copied back for the error check."""
     import torch
-    from aretomo3_b200 import recon, synth
-    dev = torch.device("cuda", local_rank)
-    torch.cuda.set_device(dev)
-    frames = synth.make_tilt_series(c["nx"], c["ny"], c["tilts"], c["vol_z"], c["phantom"])
+    from aretomo3_b200 import recon, ranks
     T, ny, nx = frames.shape
     Nx, Nz = nx & ~1, c["vol_z"]
+    dev = proj.device
     plan = recon.Plan(nx, ny, c["tilts"], Nz, **plan_kwargs(c))
     c["_c2r"] = plan.c2r
-    stream = torch.cuda.current_stream(dev)
-    proj = torch.from_numpy(frames).to(dev)
-    vol = torch.empty((ny, Nz, Nx), device=dev, dtype=torch.float32)
-
-    from aretomo3_b200 import ranks
-    barrier = ranks.barrier
-
-    def max_over_ranks(x: float) -> float:
-        return ranks.max_over_ranks(x, device=dev)
-
-    for _ in range(args.warmup):
+    out = {"slab_slices": plan.slab, "c2r": plan.c2r}
+    for _ in range(warmup):
         plan.run_device(proj.data_ptr(), vol.data_ptr(), stream.cuda_stream)
     torch.cuda.synchronize()
-
-    # timed region: device-resident, no per-launch events (a WBP plan runs its
-    # slabs on two streams here)
-    gpu_index = int(os.environ.get("CUDA_VISIBLE_DEVICES", str(local_rank)).split(",")[local_rank]) \
-        if os.environ.get("CUDA_VISIBLE_DEVICES", "").replace(",", "").isdigit() else local_rank
-    clocks = ClockSampler(gpu_index)
-    clocks.start()
-    time.sleep(0.3)
-    barrier()
+    sampler = ClockSampler(gpu_index) if clocks else None
+    if sampler:
+        sampler.start()
+        time.sleep(0.3)
+    ranks.barrier()
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
-    for _ in range(args.steps):
+    for _ in range(steps):
         plan.run_device(proj.data_ptr(), vol.data_ptr(), stream.cuda_stream)
     e1.record(stream)
     torch.cuda.synchronize()
-    barrier()
-    ms_total = max_over_ranks(e0.elapsed_time(e1))
-    clk = clocks.stop()
-    launches_per_step = plan.last_launches
-
-    # per-kernel device times: the same steps again with an event pair on the
-    # launching stream around every launch.  The plan runs one stream while
-    # timing is on, so no kernel's events also time another's work.  One step
-    # when a step takes seconds.
-    plan.set_timing(True)
-    k_steps = args.steps if ms_total / args.steps < 5000.0 else 1
-    torch.cuda.synchronize()
-    f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    f0.record(stream)
-    for _ in range(k_steps):
-        plan.run_device(proj.data_ptr(), vol.data_ptr(), stream.cuda_stream)
-    f1.record(stream)
-    torch.cuda.synchronize()
-    ms_instr = max_over_ranks(f0.elapsed_time(f1)) / k_steps
-    kstats = plan.kernel_stats()   # the last instrumented step
-    plan.set_timing(False)
-    # a volume above 8 GB is not copied back whole: the error check reads its
-    # middle slices, and the host path writes a ring of pinned frames
-    big = Nx * Nz * ny * 4 > (8 << 30)
-    y_mid = ny // 2
-    if rank != 0:
-        vol_host = None
-    elif big:
-        vol_host = None
-        vol_mid = vol[y_mid:y_mid + 2].cpu().numpy()
-    else:
-        vol_host = vol.cpu().numpy()
-
-    # e2e through the host API: pinned frames in, pinned volume frames out
-    pin_in = torch.from_numpy(frames).pin_memory()
-    ring = 64 if big else ny
-    pin_out = torch.empty((ring, Nz, Nx), dtype=torch.float32).pin_memory()
-    fin = [pin_in[t].numpy() for t in range(T)]
-    fout = [pin_out[y % ring].numpy() for y in range(ny)]
-    plan.run_host(fin, fout, stream.cuda_stream)  # warm the host-path buffers
-    torch.cuda.synchronize()
-    barrier()
-    g0, g1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    g0.record(stream)
-    for _ in range(args.steps):
-        plan.run_host(fin, fout, stream.cuda_stream)
-    g1.record(stream)
-    torch.cuda.synchronize()
-    barrier()
-    ms_e2e = max_over_ranks(g0.elapsed_time(g1))
-    host_ok = (bool(np.array_equal(pin_out.numpy(), vol_host)) if not big else None) if rank == 0 else True
-
-    # volume output stage (CTiltSeries::FlipVol): the XY-frame volume written by
-    # the host path directly, against XZ frames followed by the host-side flip
-    out_stage = None
-    if args.output == "xyz" and not big:
-        pin_xyz = torch.empty((Nz, ny, Nx), dtype=torch.float32).pin_memory()
-        xyz = pin_xyz.numpy()
-        plan.run_host_xyz(fin, out=xyz, flip=True)
-        torch.cuda.synchronize()
-        h0, h1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        h0.record(stream)
-        for _ in range(args.steps):
-            plan.run_host_xyz(fin, out=xyz, flip=True, stream=stream.cuda_stream)
-        h1.record(stream)
-        torch.cuda.synchronize()
-        ms_xyz = h0.elapsed_time(h1) / args.steps
-        # the reference's loop: one row copy per (z, y) into new frames
-        t = time.perf_counter()
-        flipped = np.empty((Nz, ny, Nx), np.float32)
-        src = pin_out.numpy()
-        for zr in range(Nz):
-            flipped[Nz - 1 - zr] = src[:, zr, :]
-        ms_flip = (time.perf_counter() - t) * 1e3
-        out_stage = {"xyz_e2e_ms_per_step": ms_xyz, "xzy_e2e_ms_per_step": ms_e2e / args.steps,
-                     "host_flipvol_ms": ms_flip, "equal": bool(np.array_equal(flipped, xyz)),
-                     "xyz_e2e_value": units_per_step(c) / (ms_xyz / 1e3) / 1e9,
-                     "note": "xyz: XY frames of FlipVol(1) written by the host path (device transpose per slab, "
-                             "one strided copy per slab); xzy + host_flipvol: XZ frames, then the reference's "
-                             "row-copy loop on one host thread"}
-
+    ranks.barrier()
+    ms_total = ranks.max_over_ranks(e0.elapsed_time(e1), device=dev)
+    out["clocks"] = sampler.stop() if sampler else None
+    out["launches_per_step"] = plan.last_launches
     units = units_per_step(c)
-    value = ranks.aggregate_rate(units, args.steps, world, ms_total) / 1e9
-    e2e_value = ranks.aggregate_rate(units, args.steps, world, ms_e2e) / 1e9
+    out["ms_per_step"] = ms_total / steps
+    out["value"] = ranks.aggregate_rate(units, steps, world, ms_total) / 1e9
+    y_mid = ny // 2
+    out["mid"] = vol[y_mid:y_mid + 2].cpu().numpy()
+    if instrument:
+        # per-kernel device times: one more step with an event pair on the
+        # launching stream around every launch (the plan runs one stream while
+        # timing is on, so no kernel's events also time another's work)
+        plan.set_timing(True)
+        torch.cuda.synchronize()
+        f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        f0.record(stream)
+        plan.run_device(proj.data_ptr(), vol.data_ptr(), stream.cuda_stream)
+        f1.record(stream)
+        torch.cuda.synchronize()
+        out["instrumented_ms"] = ranks.max_over_ranks(f0.elapsed_time(f1), device=dev)
+        out["kstats"] = plan.kernel_stats()
+        plan.set_timing(False)
+    if e2e_steps > 0:
+        # e2e through the host API: pinned frames in, pinned volume frames out
+        # (a ring of frames when the volume would not fit host memory twice)
+        big = Nx * Nz * ny * 4 > (8 << 30)
+        ring = 64 if big else ny
+        pin_in = torch.from_numpy(frames).pin_memory()
+        pin_out = torch.empty((ring, Nz, Nx), dtype=torch.float32).pin_memory()
+        fin = [pin_in[t].numpy() for t in range(T)]
+        fout = [pin_out[y % ring].numpy() for y in range(ny)]
+        plan.run_host(fin, fout, stream.cuda_stream)  # warm the host-path buffers
+        torch.cuda.synchronize()
+        ranks.barrier()
+        g0, g1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        g0.record(stream)
+        for _ in range(e2e_steps):
+            plan.run_host(fin, fout, stream.cuda_stream)
+        g1.record(stream)
+        torch.cuda.synchronize()
+        ranks.barrier()
+        ms_e2e = ranks.max_over_ranks(g0.elapsed_time(g1), device=dev)
+        # the frames the host path wrote last equal the device path's slices
+        last = torch.arange(ny - ring, ny)
+        dev_tail = vol[ny - ring:].cpu()
+        host_ok = bool(torch.equal(pin_out[last % ring], dev_tail))
+        out["e2e"] = {"value": ranks.aggregate_rate(units, e2e_steps, world, ms_e2e) / 1e9, "unit": UNIT,
+                      "ms_per_step": ms_e2e / e2e_steps, "steps": e2e_steps,
+                      "h2d_bytes_per_step": int(frames.nbytes), "d2h_bytes_per_step": int(Nx * Nz * ny * 4),
+                      "host_equals_device": host_ok,
+                      "host_frames": "one pinned frame per slice" if not big else
+                                     f"every slice copied out, into a ring of {ring} pinned frames"}
+        del pin_in, pin_out
+    plan.close()
+    return out
 
-    if rank != 0:
-        return
-    # roofline of the dominant kernel
+
+def roofline_of(kstats, c, clk) -> tuple[dict, dict]:
+    """Roofline of the kernel with the largest device time in `kstats`, and
+    the share table of every kernel."""
     peaks = measured_peaks()
-    dom = max(kstats.items(), key=lambda kv: kv[1]["ms"])
-    dname, d = dom
+    dname, d = max(kstats.items(), key=lambda kv: kv[1]["ms"])
     per_launch_bytes = d["bytes"] / d["launches"]
     per_launch_ms = d["ms"] / d["launches"]
     achieved = per_launch_bytes / (per_launch_ms / 1e3) / 1e9
@@ -414,45 +405,181 @@ def run_our_arm(args, c, rank, world, local_rank):
             "traffic": profiled_traffic(dname, c["name"], c["storage"]),
             "bytes_per_launch": per_launch_bytes, "ms_per_launch": per_launch_ms,
             "units_per_s": d["units"] / (d["ms"] / 1e3),
-            "onchip": onchip_roof(dname, d, c["storage"], clk)}
-    step_ms = ms_total / args.steps
-    kernel_share = {k: {"launches": v["launches"], "ms": round(v["ms"], 3),
-                        "share": round(v["ms"] / max(sum(x["ms"] for x in kstats.values()), 1e-9), 4),
-                        "GB_per_s": round(v["bytes"] / max(v["ms"], 1e-9) / 1e6, 1),
-                        "Gunits_per_s": round(v["units"] / max(v["ms"], 1e-9) / 1e6, 1)}
-                    for k, v in kstats.items()}
+            "onchip": onchip_roof(dname, d, c["storage"], clk or {})}
+    tot = max(sum(x["ms"] for x in kstats.values()), 1e-9)
+    share = {k: {"launches": v["launches"], "ms": round(v["ms"], 3), "share": round(v["ms"] / tot, 4),
+                 "GB_per_s": round(v["bytes"] / max(v["ms"], 1e-9) / 1e6, 1),
+                 "Gunits_per_s": round(v["units"] / max(v["ms"], 1e-9) / 1e6, 1)}
+             for k, v in kstats.items()}
+    return roof, share
+
+
+def oracle_mid(c, frames, c2r) -> np.ndarray:
+    """The FP64 oracle's two middle slices of the series (the checker)."""
+    ol = _oracle()
+    y0 = c["ny"] // 2
+    threads = os.cpu_count() or 1
+    if c["method"] == "sart":
+        return ol.sart(frames, c["tilts"], c["vol_z"], 0, len(c["tilts"]), c["iters"], c["subsets"],
+                       relax=c.get("relax", 0.0), y0=y0, y1=y0 + 2, threads=threads)
+    from aretomo3_b200 import recon
+    return ol.wbp(frames, c["tilts"], c["vol_z"], y0=y0, y1=y0 + 2, c2r_mode=1 if c2r == recon.C2R_PACKED else 0,
+                  threads=threads)
+
+
+def err_of(got, ref) -> dict:
+    g = got.astype(np.float64)
+    return {"rel_l2": float(np.linalg.norm(g - ref) / np.linalg.norm(ref)), "max_abs": float(np.abs(g - ref).max()),
+            "slices": int(got.shape[0]), "against": "FP64 oracle"}
+
+
+def reference_cuda(c_sart, c_wbp, frames) -> dict:
+    """The reference's own CUDA Recon (CDoWbpRecon::DoIt / CDoSartRecon::DoIt,
+    built from its sources for sm_100a into oracle/_ref/ref_recon) against this
+    library's reference-shaped entry points (recon.CDoWbpRecon / CDoSartRecon:
+    a new plan per call, pageable host frames in and out, as CTiltSeries holds
+    them) on a band of rows of the same series (every y-slice is independent):
+    wall time of each DoIt (median of three after a warm-up for ours, the
+    reference's own timer around its DoIt), and the relative L2 between the two
+    volumes."""
+    sys.path.insert(0, os.path.join(ROOT, "tests", "golden"))
+    import gen_golden  # noqa: E402  (runs the reference binary)
+    from aretomo3_b200 import recon
+    if not os.path.exists(gen_golden.REF_BIN):
+        return {"unavailable": "oracle/_ref/ref_recon was not built (the reference tree was absent at build time)"}
+    out = {}
+    for c, rows in ((c_wbp, 256), (c_sart, 32)):
+        y0 = c["ny"] // 2 - rows // 2
+        band = np.ascontiguousarray(frames[:, y0:y0 + rows, :])
+        T, ny, nx = band.shape
+        if c["method"] == "sart":
+            ref, info = gen_golden.run_reference("sart", band, c["tilts"], c["vol_z"], 0, T, c["iters"], c["subsets"])
+        else:
+            ref, info = gen_golden.run_reference("wbp", band, c["tilts"], c["vol_z"])
+        ts = recon.TiltSeries(band)
+        ap = recon.AlignParam(np.asarray(c["tilts"], np.float32))
+
+        def ours():
+            if c["method"] == "sart":
+                return recon.CDoSartRecon().DoIt(ts, ap, 0, T, c["vol_z"], c["iters"], c["subsets"])
+            return recon.CDoWbpRecon().DoIt(ts, ap, c["vol_z"])
+        ours()
+        times = []
+        for _ in range(3):
+            t = time.perf_counter()
+            vol = ours()
+            times.append(time.perf_counter() - t)
+        t_ours = float(np.median(times))
+        units = float(nx & ~1) * ny * c["vol_z"] * T
+        out[c["method"]] = {
+            "rows": [int(y0), int(y0 + rows)], "reference_s": info["seconds"], "ours_s": t_ours,
+            "reference_value": units / info["seconds"] / 1e9, "ours_value": units / t_ours / 1e9, "unit": UNIT,
+            "speedup": info["seconds"] / t_ours,
+            "rel_l2_vs_reference": float(np.linalg.norm(vol.astype(np.float64) - ref) /
+                                         np.linalg.norm(ref.astype(np.float64)))}
+    out["note"] = ("pageable host frames in, host XZ frames out on both sides; the reference's DoIt has no "
+                   "relaxation argument (1/subsets), as this workload's SART")
+    return out
+
+
+def run_our_arm(args, c, rank, world, local_rank):
+    import torch
+    from aretomo3_b200 import synth
+    dev = torch.device("cuda", local_rank)
+    torch.cuda.set_device(dev)
+    frames = synth.make_tilt_series(c["nx"], c["ny"], c["tilts"], c["vol_z"], c["phantom"])
+    T, ny, nx = frames.shape
+    Nx, Nz = nx & ~1, c["vol_z"]
+    stream = torch.cuda.current_stream(dev)
+    proj = torch.from_numpy(frames).to(dev)
+    vol = torch.empty((ny, Nz, Nx), device=dev, dtype=torch.float32)
+    gpu_index = _gpu_index(local_rank)
+    e2e_steps = args.steps if args.e2e_steps <= 0 else min(args.steps, args.e2e_steps)
+    m = measure(c, frames, proj, vol, stream, args.steps, args.warmup, e2e_steps, world, gpu_index)
+    clk = m["clocks"]
+    sub = {}
+    full = rank == 0 and world == 1 and not args.no_cpu_baseline
+    if c.get("with_wbp") and world == 1:
+        # the metric's WBP half on the same series
+        cw = dict(c, method="wbp", name=c["name"] + "_wbp", label=c["wbp_label"])
+        w = measure(cw, frames, proj, vol, stream, min(args.steps, 5), 2, min(args.steps, 2), world, gpu_index,
+                    clocks=True)
+        sub["wbp"] = (cw, w)
+    prec = {}
+    if c.get("with_precision") and world == 1:
+        # the reduced-precision form beside the FP32 path, WBP and SART
+        for st in ("f16", "bf16"):
+            for meth, base in (("sart", (c, m)), ("wbp", sub.get("wbp"))):
+                if base is None:
+                    continue
+                cc = dict(base[0], storage=st)
+                r = measure(cc, frames, proj, vol, stream, min(args.steps, 2 if meth == "sart" else 3), 1, 0,
+                            world, gpu_index, instrument=False, clocks=False)
+                prec[f"{meth}_{st}"] = (cc, r, base[1])
+    if rank != 0:
+        return
+    roof, share = roofline_of(m["kstats"], c, clk)
+    units = units_per_step(c)
     line = {
-        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f32" if c["storage"] == "f32" else f"{c['storage']}-storage/f32-accumulate",
+        "metric": METRIC, "value": m["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": m["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32" if c["storage"] == "f32" else f"{c['storage']}-storage/f32-accumulate",
         "data": "synthetic",
-        "config": {"workload": c["label"], "name": c["name"], "storage": c["storage"], "nx": nx, "ny": ny, "tilts": T, "vol_z": Nz,
-                   "units_per_step": units, "slab_slices": plan.slab,
-                   "l2": "inputs larger than L2 (projections 256 MB, volume 1.26 GB at the default workload)",
+        "config": {"workload": c["label"], "name": c["name"], "storage": c["storage"], "nx": nx, "ny": ny,
+                   "tilts": T, "vol_z": Nz, "units_per_step": units, "slab_slices": m["slab_slices"],
+                   "step": "one full reconstruction of the series",
+                   "l2": f"inputs larger than L2 (projections {frames.nbytes / 1e6:.0f} MB, volume "
+                         f"{Nx * Nz * ny * 4 / 1e9:.2f} GB)",
                    "parallelism": f"replicas x{world}"},
-        "e2e": {"value": e2e_value, "unit": UNIT, "ms_per_step": ms_e2e / args.steps,
-                "h2d_bytes_per_step": int(frames.nbytes), "d2h_bytes_per_step": int(Nx * Nz * ny * 4),
-                "host_equals_device": host_ok,
-                "host_frames": "one pinned frame per slice" if not big else
-                               f"every slice copied out, into a ring of {ring} pinned frames"},
-        "gpu_launches": int(launches_per_step * args.steps),
+        "e2e": m.get("e2e"),
+        "gpu_launches": int(m["launches_per_step"] * args.steps),
         "roofline": roof,
-        "kernels": kernel_share,
-        "instrumented": {"ms_per_step": ms_instr, "steps": k_steps,
-                         "overhead": ms_instr / step_ms - 1.0,
-                         "note": "per-kernel events, one stream; the kernels and roofline come from these steps"},
-        "output_stage": out_stage,
+        "kernels": share,
+        "instrumented": {"ms_per_step": m["instrumented_ms"], "steps": 1,
+                         "overhead": m["instrumented_ms"] / m["ms_per_step"] - 1.0,
+                         "note": "per-kernel events, one stream; the kernels and roofline come from this step"},
         "clocks": clk,
     }
-    if not args.no_cpu_baseline and world == 1:
+    refs = {}
+    if full:
         threads = os.cpu_count() or 1
         line["cpu_baseline"] = cpu_baseline(c, frames, threads)
-        if big:
-            line["error"] = error_vs_oracle(c, frames, None, mid=vol_mid)
-        else:
-            line["error"] = error_vs_oracle(c, frames, vol_host)
+        refs["sart" if c["method"] == "sart" else "wbp"] = oracle_mid(c, frames, m["c2r"])
+        line["error"] = err_of(m["mid"], refs[c["method"]])
+    if "wbp" in sub:
+        cw, w = sub["wbp"]
+        wroof, wshare = roofline_of(w["kstats"], cw, w["clocks"])
+        rec = {"value": w["value"], "unit": UNIT, "ms_per_step": w["ms_per_step"], "steps": min(args.steps, 5),
+               "warmup": 2, "workload": cw["label"], "units_per_step": units_per_step(cw),
+               "slab_slices": w["slab_slices"], "e2e": w.get("e2e"), "roofline": wroof, "kernels": wshare,
+               "gpu_launches": int(w["launches_per_step"] * min(args.steps, 5)), "clocks": w["clocks"]}
+        if full:
+            refs["wbp"] = oracle_mid(cw, frames, w["c2r"])
+            rec["error"] = err_of(w["mid"], refs["wbp"])
+            base = dict(cw, storage="f32")
+            rec["cpu_baseline"] = cpu_baseline(base, frames, os.cpu_count() or 1)
+        line["wbp"] = rec
+    if prec:
+        pr = {}
+        for k, (cc, r, b) in prec.items():
+            e = {"value": r["value"], "unit": UNIT, "ms_per_step": r["ms_per_step"],
+                 "speedup_vs_f32": r["value"] / b["value"], "storage": cc["storage"],
+                 "steps": min(args.steps, 2 if cc["method"] == "sart" else 3), "warmup": 1}
+            if cc["method"] in refs:
+                e["error"] = err_of(r["mid"], refs[cc["method"]])
+                e["error_f32"] = err_of(b["mid"], refs[cc["method"]])
+                e["within_1e-3"] = e["error"]["rel_l2"] <= 1e-3
+            pr[k] = e
+        pr["note"] = ("filtered projections (WBP) or weighted projections and residual (SART) stored as 16-bit "
+                      "values with one FP32 scale per (slice, tilt) row; SART also reads a 16-bit shadow of its "
+                      "working volume in the forward projection; accumulation FP32; bound 1e-3 relative L2 "
+                      "against the FP64 oracle")
+        line["precision"] = pr
+    if full and c.get("with_reference_cuda"):
+        cw = sub["wbp"][0] if "wbp" in sub else dict(c, method="wbp")
+        line["reference_cuda"] = reference_cuda(c, cw, frames)
     print(json.dumps(line), flush=True)
-    plan.close()
 
 
 # --- batched form: many uneven series in one graph launch --------------------
@@ -895,7 +1022,9 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="sart_1k")
+    ap.add_argument("--workload", default="recon_4k")
+    ap.add_argument("--e2e-steps", type=int, default=3,
+                    help="steps of the host-API (e2e) measurement, at most --steps (0: --steps)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--storage", default="f32", choices=sorted(STORAGE),
                     help="staged-sinogram storage: f32, or f16 / bf16 with per-tilt scale (FP32 accumulation)")
