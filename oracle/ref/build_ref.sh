@@ -44,6 +44,22 @@ $NVCC -gencode arch=compute_100a,code=sm_100a -o "$OUT/ref_recon" "${objs[@]}" \
   "$OBJ/ref_stub.o" "$OBJ/ref_driver.o" -lcufft -lcurand -lcuda
 echo "built $OUT/ref_recon"
 
+# the drop-in shim (integration/at3r_recon_shim.cpp: CDoWbpRecon / CDoSartRecon
+# with their bodies calling libat3r) linked in place of the reference's
+# CDoWbpRecon.cpp / CDoSartRecon.cpp, with the same driver: oracle/_ref/shim_recon
+LIBDIR="$HERE/../../aretomo3_b200"
+if [ -f "$LIBDIR/libat3r.so" ]; then
+  g++ $CXXFLAGS -I"$HERE/../../include" -c "$HERE/../../integration/at3r_recon_shim.cpp" -o "$OBJ/at3r_recon_shim.o"
+  sh=()
+  for o in "${objs[@]}"; do
+    case "$o" in *AreTomo_Recon_CDoWbpRecon.o|*AreTomo_Recon_CDoSartRecon.o) ;; *) sh+=("$o") ;; esac
+  done
+  $NVCC -gencode arch=compute_100a,code=sm_100a -o "$OUT/shim_recon" "${sh[@]}" "$OBJ/at3r_recon_shim.o" \
+    "$OBJ/ref_stub.o" "$OBJ/ref_driver.o" -L"$LIBDIR" -lat3r -Xlinker -rpath -Xlinker '$ORIGIN/../../aretomo3_b200' \
+    -lcufft -lcurand -lcuda
+  echo "built $OUT/shim_recon"
+fi
+
 # the projection-alignment re-projector (AreTomo/ProjAlign/GReproj.cu + CCalcReproj.cpp)
 rp=()
 for f in AreTomo/ProjAlign/GReproj; do
