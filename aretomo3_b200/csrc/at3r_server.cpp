@@ -38,6 +38,7 @@ struct Request {
     at3r_status status = AT3R_OK;
     std::string err;
     bool done = false;
+    bool waited = false;   // a caller is in at3r_server_wait for it (one waiter per request)
 };
 
 }  // namespace
@@ -173,6 +174,11 @@ at3r_status at3r_server_wait(at3r_server* s, int64_t id, double* latency_s, doub
         return AT3R_ERR_INVALID_ARGUMENT;
     }
     Request* r = it->second;
+    if (r->waited) {
+        at3r_set_last_error("another thread is already waiting for this request");
+        return AT3R_ERR_INVALID_ARGUMENT;
+    }
+    r->waited = true;
     s->cv.wait(lk, [r] { return r->done; });
     if (latency_s) *latency_s = std::chrono::duration<double>(r->t_done - r->t_submit).count();
     if (queued_s) *queued_s = std::chrono::duration<double>(r->t_start - r->t_submit).count();

@@ -167,54 +167,78 @@ inline void bind_fft(HostFft& h)
 // Which convention does the system cuFFT use for a 2-D C2R of (nz x nx)?
 // A pure-imaginary DC bin is invisible under the Hermitian reading and shows
 // up as -1/+1 on even/odd samples under half-length packing.  libcufft is
-// opened at run time, only for this question, once per size.
+// opened at run time, only for this question, once per size and process.
+// The probe runs on a stream of its own with stream-ordered memory and keeps
+// its cuFFT plan (destroying one frees cuFFT's tables with a cudaFree, which
+// would wait for the whole device), so it never synchronises other streams.
+// *measured (may be null) tells whether cuFFT answered; when it cannot be
+// loaded the Hermitian reading is assumed.
 // ---------------------------------------------------------------------------
-inline int probe_cufft_c2r(int nz, int nx)
+inline int probe_cufft_c2r(int nz, int nx, bool* measured = nullptr)
 {
     static std::mutex mu;
-    static std::map<std::pair<int, int>, int> cache;
+    static std::map<std::pair<int, int>, std::pair<int, bool>> cache;
     std::lock_guard<std::mutex> lk(mu);
     auto key = std::make_pair(nz, nx);
     auto it = cache.find(key);
-    if (it != cache.end()) return it->second;
-    int result = AT3R_C2R_HERMITIAN;
+    if (it != cache.end()) {
+        if (measured) *measured = it->second.second;
+        return it->second.first;
+    }
+    typedef int (*create_t)(int*);
+    typedef int (*setauto_t)(int, int);
+    typedef int (*make2d_t)(int, int, int, int, size_t*);
+    typedef int (*setwork_t)(int, void*);
+    typedef int (*setstream_t)(int, cudaStream_t);
+    typedef int (*exec_t)(int, void*, float*);
     static void* lib = nullptr;
-    if (!lib) {
+    static bool tried = false;
+    if (!tried) {
+        tried = true;
         for (const char* name : {"/usr/local/cuda/lib64/libcufft.so.11", "libcufft.so.11", "libcufft.so.12", "libcufft.so"}) {
             lib = dlopen(name, RTLD_NOW | RTLD_LOCAL);
             if (lib) break;
         }
     }
+    int result = AT3R_C2R_HERMITIAN;
+    bool ok = false;
     if (lib) {
-        typedef int (*plan2d_t)(int*, int, int, int);
-        typedef int (*exec_t)(int, void*, float*);
-        typedef int (*destroy_t)(int);
-        auto plan2d = (plan2d_t)dlsym(lib, "cufftPlan2d");
+        auto create = (create_t)dlsym(lib, "cufftCreate");
+        auto setauto = (setauto_t)dlsym(lib, "cufftSetAutoAllocation");
+        auto make2d = (make2d_t)dlsym(lib, "cufftMakePlan2d");
+        auto setwork = (setwork_t)dlsym(lib, "cufftSetWorkArea");
+        auto setstream = (setstream_t)dlsym(lib, "cufftSetStream");
         auto exec = (exec_t)dlsym(lib, "cufftExecC2R");
-        auto destroy = (destroy_t)dlsym(lib, "cufftDestroy");
-        if (plan2d && exec && destroy) {
-            const int kx = nx / 2 + 1;
-            const size_t elems = (size_t)nz * kx;
-            float2* d = nullptr;
-            if (cudaMalloc(&d, elems * sizeof(float2)) == cudaSuccess) {
-                cudaMemset(d, 0, elems * sizeof(float2));
-                const float2 one_i = make_float2(0.f, 1.f);
-                cudaMemcpy(d, &one_i, sizeof(float2), cudaMemcpyHostToDevice);
-                int plan = 0;
-                if (plan2d(&plan, nz, nx, 0x2c /* CUFFT_C2R */) == 0) {
-                    if (exec(plan, d, reinterpret_cast<float*>(d)) == 0) {
-                        float o[2] = {0.f, 0.f};
-                        cudaMemcpy(o, d, sizeof(o), cudaMemcpyDeviceToHost);
-                        if (std::fabs(o[0]) > 0.5f) result = AT3R_C2R_PACKED;
-                    }
-                    destroy(plan);
+        cudaStream_t st = nullptr;
+        int plan = 0;
+        size_t work = 0;
+        if (create && setauto && make2d && setwork && setstream && exec &&
+            cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) == cudaSuccess && create(&plan) == 0 &&
+            setauto(plan, 0) == 0 && make2d(plan, nz, nx, 0x2c /* CUFFT_C2R */, &work) == 0) {
+            const size_t elems = (size_t)nz * (nx / 2 + 1);
+            const size_t data_bytes = (elems * sizeof(float2) + 255) / 256 * 256;
+            char* d = nullptr;
+            if (cudaMallocAsync(reinterpret_cast<void**>(&d), data_bytes + work, st) == cudaSuccess) {
+                static const float2 one_i = make_float2(0.f, 1.f);
+                float o[2] = {0.f, 0.f};
+                if (cudaMemsetAsync(d, 0, elems * sizeof(float2), st) == cudaSuccess &&
+                    cudaMemcpyAsync(d, &one_i, sizeof(float2), cudaMemcpyHostToDevice, st) == cudaSuccess &&
+                    setwork(plan, work ? d + data_bytes : nullptr) == 0 && setstream(plan, st) == 0 &&
+                    exec(plan, d, reinterpret_cast<float*>(d)) == 0 &&
+                    cudaMemcpyAsync(o, d, sizeof(o), cudaMemcpyDeviceToHost, st) == cudaSuccess &&
+                    cudaStreamSynchronize(st) == cudaSuccess) {
+                    ok = true;
+                    if (std::fabs(o[0]) > 0.5f) result = AT3R_C2R_PACKED;
                 }
-                cudaFree(d);
+                cudaFreeAsync(d, st);
+                cudaStreamSynchronize(st);
             }
-            cudaGetLastError();
         }
+        if (st) cudaStreamDestroy(st);
+        cudaGetLastError();
     }
-    cache[key] = result;
+    cache[key] = {result, ok};
+    if (measured) *measured = ok;
     return result;
 }
 

@@ -102,23 +102,32 @@ at3r_status at3r_mrc_write(const char* path, const float* const* frames, int nx,
     unsigned char header[1024];
     mrc_header(header, nx, ny, nz, pix_size);
     bool ok = pwrite_all(fd, header, sizeof(header), 0);
-    // frames at 1024 + z * frame bytes, split over up to four writer threads
+    int err = ok ? 0 : errno;
+    // frames at 1024 + z * frame bytes, split over up to four writer threads;
+    // each thread keeps the errno of its own failed write (errno is per thread)
     const size_t fbytes = (size_t)nx * ny * sizeof(float);
     const int nt = (int)std::max(1, std::min(4, nz));
-    std::vector<char> okt(nt, 1);
-    auto run = [&](int k) {
-        for (int z = k; z < nz && okt[k]; z += nt)
-            okt[k] = pwrite_all(fd, frames[z], fbytes, (off_t)(1024 + (size_t)z * fbytes)) ? 1 : 0;
+    std::vector<int> errt(nt, 0);
+    auto run = [&](int k, int stride) {
+        for (int z = k; z < nz && !errt[k]; z += stride)
+            if (!pwrite_all(fd, frames[z], fbytes, (off_t)(1024 + (size_t)z * fbytes))) errt[k] = errno ? errno : EIO;
     };
     if (ok) {
         std::vector<std::thread> th;
-        for (int k = 1; k < nt; k++) th.emplace_back(run, k);
-        run(0);
+        try {
+            for (int k = 1; k < nt; k++) th.emplace_back(run, k, nt);
+        } catch (const std::exception&) {
+            // no threads to be had: the frames the missing threads would have
+            // written are written here, after the calling thread's own share
+        }
+        const int started = 1 + (int)th.size();
+        run(0, nt);
+        for (int k = started; k < nt; k++) run(k, nt);
         for (std::thread& t : th) t.join();
-        for (char c : okt) ok = ok && c;
+        for (int e : errt)
+            if (e && ok) { ok = false; err = e; }
     }
-    const int err = errno;
-    if (close(fd) != 0) ok = false;
+    if (close(fd) != 0 && ok) { ok = false; err = errno; }
     if (!ok) return mrc_err(AT3R_ERR_IO, std::string("write to ") + path + " failed: " + std::strerror(err));
     return AT3R_OK;
 }

@@ -665,7 +665,11 @@ at3r_status at3r_stack_create(const at3r_stack_geom* g, at3r_stack** out)
 
     // FFT plans of the binning (row length ax, column lengths ay -> by, C2R length bx)
     if (!s->same) {
-        s->c2r = probe_cufft_c2r(s->by, s->bx);
+        bool measured = false;
+        s->c2r = probe_cufft_c2r(s->by, s->bx, &measured);
+        if (!measured)
+            return fail(st_err(AT3R_ERR_UNSUPPORTED, "cannot ask cuFFT which C2R convention it uses for the "
+                                                     "binned size (libcufft not loadable)"));
         if ((rc = make_fft_tables(s->ax, s->frow)) || (rc = make_fft_tables(s->ay, s->fcin)) ||
             (rc = make_fft_tables(s->by, s->fcout)) || (rc = make_fft_tables(s->bx, s->fbx)))
             return fail(rc);
