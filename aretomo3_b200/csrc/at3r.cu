@@ -10,6 +10,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <ctime>
 #include <complex>
 #include <cstdio>
 #include <cstring>
@@ -86,6 +87,8 @@ struct at3r_plan {
     void* d_shadow = nullptr;   // 16-bit storage: the volume shadow the forward projector reads
     float4* d_w = nullptr;      // SART working volume, slice groups [ceil(S/4)][Nz][Nx] x 4 slices
     int* d_flags = nullptr;
+    int* d_seen = nullptr;                 // run summary: every slice's flag bits ORed in
+    unsigned long long fill_seed = 0;      // seed of the empty-voxel fill's random table
     double* d_rf = nullptr;
     std::vector<double> h_rf;
     // WBP
@@ -319,11 +322,13 @@ at3r_status run_slab_t(at3r_plan* p, const float* proj, size_t tilt_stride, int 
         // the working volume in slice groups: one 16-byte (or 8-byte shadow)
         // load gives a tap of four slices; unpacked into vol at the end
         AT3R_CUDA(cudaMemsetAsync(p->d_w, 0, sizeof(float4) * (size_t)SG * Nx * Nz, st));
-        if (p->d_shadow) AT3R_CUDA(cudaMemsetAsync(p->d_shadow, 0, sizeof(uint2) * (size_t)SG * Nx * Nz, st));
+        // the 16-bit shadow: eight slices per voxel
+        const int SG8 = (S + 7) / 8;
+        if (p->d_shadow) AT3R_CUDA(cudaMemsetAsync(p->d_shadow, 0, sizeof(uint4) * (size_t)SG8 * Nx * Nz, st));
         BpArgs a{};
         a.T = T; a.N = N; a.cs = p->d_cs; a.GX = Nx; a.GZ = Nz; a.S = S;
         a.out = reinterpret_cast<float*>(p->d_w); a.out_slice = (size_t)Nx * Nz; a.ww = p->bp_ww_sart;
-        a.flags = p->d_flags;
+        a.flags = p->d_flags; a.seen = p->d_seen;
         a.scale = p->d_scale; a.shadow = p->d_shadow;
         const dim3 bgrid((Nx + BP_TX - 1) / BP_TX, (Nz + BP_TZ - 1) / BP_TZ, SG);
         // first back-projection: all tilts, relax 1 (CTomoSart.cpp:68-69)
@@ -340,7 +345,8 @@ at3r_status run_slab_t(at3r_plan* p, const float* proj, size_t tilt_stride, int 
                 for (int t = t0; t < t0 + nt; t++) samples += (double)p->ray_len[t];
                 double* rfp = p->g.compute_rfactor ? p->d_rf + 2 * it : nullptr;
                 TB(p, st);
-                k_fp_diff<ST, VT, true><<<dim3((N + 255) / 256, nt, SG), 256, 0, st>>>(
+                k_fp_diff<ST, VT, true><<<dim3((N + 255) / 256, nt, (S + fp_slices<VT>() - 1) / fp_slices<VT>()), 256,
+                                          0, st>>>(
                     reinterpret_cast<const float*>(p->d_w), p->d_shadow, Nx, Nz, S, raw, dif, p->d_scale, p->d_cs, T,
                     N, t0, rfp, p->d_flags);
                 TE(p, st, KK_FP_DIFF, vs * vox + 2.0 * es * S * nt * N, samples * N * S);
@@ -354,8 +360,13 @@ at3r_status run_slab_t(at3r_plan* p, const float* proj, size_t tilt_stride, int 
         k_ungroup<<<dim3((unsigned)(((size_t)Nx * Nz + 255) / 256), SG), 256, 0, st>>>(p->d_w, vol, S,
                                                                                        (size_t)Nx * Nz);
         TE(p, st, KK_UNGROUP, 2 * f4 * vox, vox);
+        // the empty-voxel fill (CTomoSart.cpp:88); only flagged slices do work
+        const int fb = std::max(1, std::min((Nx * Nz + 255) / 256, (8 * 148 + S - 1) / S));
         TB(p, st);
-        k_fill_empty<<<S, 256, 0, st>>>(vol, (size_t)Nx * Nz, p->d_flags);
+        k_fill_mark<<<dim3(fb, S), 256, 0, st>>>(vol, Nx, Nz, p->d_flags, p->fill_seed, p->d_seen);
+        TE(p, st, KK_FILL, f4 * S, 0);
+        TB(p, st);
+        k_fill_finish<<<S, 512, 0, st>>>(vol, Nx, Nz, p->d_flags, p->d_seen);
         TE(p, st, KK_FILL, f4 * S, 0);
         return AT3R_OK;
     }
@@ -371,7 +382,7 @@ at3r_status run_slab_t(at3r_plan* p, const float* proj, size_t tilt_stride, int 
     BpArgs a{};
     a.sino = filt; a.scale = scale; a.shadow = nullptr; a.T = T; a.N = N; a.t0 = 0; a.t1 = T; a.cs = p->d_cs;
     a.GX = 2 * Nx; a.GZ = 2 * Nz; a.S = S; a.relax = 1.f; a.out = g2; a.out_slice = (size_t)4 * Nx * Nz;
-    a.ww = p->bp_ww_wbp; a.flags = flags; a.low_bit = kFlagRawLow;
+    a.ww = p->bp_ww_wbp; a.flags = flags; a.seen = p->d_seen; a.low_bit = kFlagRawLow;
     const dim3 bgrid((2 * Nx + BP_TX - 1) / BP_TX, (2 * Nz + BP_TZ - 1) / BP_TZ, SG);
     TB(p, st);
     k_bp<1, ST, float, false><<<bgrid, BP_THREADS, bp_smem(T, a.ww), st>>>(a);
@@ -435,6 +446,7 @@ at3r_status begin_run(at3r_plan* p, cudaStream_t st)
     int dev = -1;
     AT3R_CUDA(cudaGetDevice(&dev));
     if (dev != p->device) return set_err(AT3R_ERR_INVALID_ARGUMENT, "plan was created on another device");
+    AT3R_CUDA(cudaMemsetAsync(p->d_seen, 0, sizeof(int), st));
     if (p->g.method == AT3R_SART && p->g.compute_rfactor)
         AT3R_CUDA(cudaMemsetAsync(p->d_rf, 0, sizeof(double) * 2 * std::max(1, p->g.iterations), st));
     return AT3R_OK;
@@ -468,6 +480,7 @@ void at3r_geom_init(at3r_geom* g, int method)
     g->relax = 0.f;
     g->storage = AT3R_STORE_F32;
     g->c2r = AT3R_C2R_MATCH_CUFFT;
+    g->fill_seed = (unsigned long long)time(nullptr);   // as GGenRandoms::DoIt seeds it
 }
 
 at3r_status plan_create_impl(const at3r_geom* g, cudaStream_t alloc_stream, at3r_plan** out);
@@ -517,7 +530,7 @@ size_t at3r_plan_estimate_bytes(const at3r_geom* g)
     slab = std::min<size_t>(slab, (size_t)g->ny);
     size_t work;
     if (g->method == AT3R_SART)
-        work = (slab + 3) * (2 * T * N * esz + 4 * Nx * Nz + (esz < 4 ? 2 * Nx * Nz + T * 4 : 0)) + slab * 8;
+        work = (slab + 7) * (2 * T * N * esz + 4 * Nx * Nz + (esz < 4 ? 2 * Nx * Nz + T * 4 : 0)) + slab * 8;
     else   // two lanes of slab workspace when the series has more than one slab (device path)
         work = (slab < (size_t)g->ny ? 2 : 1) *
                slab * (T * N * esz + 16 * Nx * Nz + 2 * Nz * KX * sizeof(float2) + (esz < 4 ? T * 4 : 0) + 4);
@@ -556,6 +569,7 @@ at3r_status plan_create_impl(const at3r_geom* g, cudaStream_t alloc_stream, at3r
     p->tilts.assign(g->tilts_deg, g->tilts_deg + g->n_tilts);
     p->g.tilts_deg = p->tilts.data();
     p->nx = g->nx; p->ny = g->ny; p->T = g->n_tilts;
+    p->fill_seed = g->fill_seed;
     p->N = g->nx & ~1; p->Nx = p->N; p->Nz = g->vol_z; p->KX = p->Nx / 2 + 1;
     cudaGetDevice(&p->device);
 
@@ -575,6 +589,7 @@ at3r_status plan_create_impl(const at3r_geom* g, cudaStream_t alloc_stream, at3r
     auto fail = [&](at3r_status s) { at3r_plan_destroy(p); return s; };
     at3r_status rc;
     if ((rc = dalloc(p, &p->d_cs, p->T))) return fail(rc);
+    if ((rc = dalloc(p, &p->d_seen, 1))) return fail(rc);
     if (cudaMemcpy(p->d_cs, cs.data(), sizeof(float) * 2 * p->T, cudaMemcpyHostToDevice) != cudaSuccess)
         return fail(set_err(AT3R_ERR_CUDA, "geometry upload failed"));
 
@@ -595,7 +610,17 @@ at3r_status plan_create_impl(const at3r_geom* g, cudaStream_t alloc_stream, at3r
             if ((rc = set_smem(fn, bp_smem(p->T, p->bp_ww_sart)))) return fail(rc);
         per_slice = 2 * T * N * p->esz + 4 * Nx * Nz + (p->esz < 4 ? 2 * Nx * Nz + 4 * T : 0);
     } else {
-        p->c2r = g->c2r == AT3R_C2R_MATCH_CUFFT ? probe_cufft_c2r(p->Nz, p->Nx) : g->c2r;
+        if (g->c2r == AT3R_C2R_MATCH_CUFFT) {
+            bool measured = false;
+            p->c2r = probe_cufft_c2r(p->Nz, p->Nx, &measured);
+            if (!measured)
+                return fail(set_err(AT3R_ERR_UNSUPPORTED,
+                                    "cannot ask cuFFT which C2R convention it uses for " + std::to_string(p->Nz) +
+                                        " x " + std::to_string(p->Nx) +
+                                        " (libcufft not loadable); pass c2r = AT3R_C2R_HERMITIAN or AT3R_C2R_PACKED"));
+        } else {
+            p->c2r = g->c2r;
+        }
         if ((rc = make_fft(p, p->N, p->fN))) return fail(rc);
         if ((rc = make_fft(p, 2 * p->Nx, p->f2x))) return fail(rc);
         if ((rc = make_fft(p, 2 * p->Nz, p->f2z))) return fail(rc);
@@ -660,8 +685,8 @@ at3r_status plan_create_impl(const at3r_geom* g, cudaStream_t alloc_stream, at3r
         if ((rc = dalloc_bytes(p, &p->d_diff, S * T * N * p->esz))) return fail(rc);
         if (g->storage != AT3R_STORE_F32) {
             if ((rc = dalloc(p, &p->d_scale, S * T))) return fail(rc);
-            // slice pairs of 16-bit values, the slab rounded up to whole SB groups
-            if ((rc = dalloc_bytes(p, &p->d_shadow, sizeof(uint2) * ((S + SB - 1) / SB) * Nx * Nz))) return fail(rc);
+            // eight 16-bit slices per voxel, the slab rounded up to whole groups of eight
+            if ((rc = dalloc_bytes(p, &p->d_shadow, sizeof(uint4) * ((S + 7) / 8) * Nx * Nz))) return fail(rc);
         }
         if ((rc = dalloc_bytes(p, reinterpret_cast<void**>(&p->d_w), sizeof(float4) * ((S + SB - 1) / SB) * Nx * Nz)))
             return fail(rc);
@@ -684,7 +709,7 @@ void at3r_plan_destroy(at3r_plan* p)
     if (!p) return;
     // like cudaFree, wait for work that may still use the plan's memory
     if (p->pooled) cudaDeviceSynchronize();
-    for (void* ptr : {(void*)p->d_cs, (void*)p->d_raw, (void*)p->d_diff, (void*)p->d_scale, (void*)p->d_shadow,
+    for (void* ptr : {(void*)p->d_cs, (void*)p->d_seen, (void*)p->d_raw, (void*)p->d_diff, (void*)p->d_scale, (void*)p->d_shadow,
                       (void*)p->d_w,
                       (void*)p->d_flags, (void*)p->d_rf, (void*)p->d_h, (void*)p->d_filt, (void*)p->d_g2,
                       (void*)p->d_y})
@@ -1187,6 +1212,33 @@ int64_t at3r_plan_last_launches(const at3r_plan* p) { return p ? p->launches : 0
 
 int at3r_plan_c2r(const at3r_plan* p) { return p ? p->c2r : 0; }
 
+int at3r_plan_flags_seen(const at3r_plan* p)
+{
+    if (!p) return 0;
+    int v = 0;
+    if (cudaDeviceSynchronize() != cudaSuccess || cudaMemcpy(&v, p->d_seen, sizeof(int), cudaMemcpyDeviceToHost) !=
+                                                      cudaSuccess) {
+        cudaGetLastError();
+        return -1;
+    }
+    return v;
+}
+
+at3r_status at3r_plan_fill_table(const at3r_plan* p, int* table, size_t n)
+{
+    if (!p || !table) return set_err(AT3R_ERR_INVALID_ARGUMENT, "null argument");
+    if (p->g.method != AT3R_SART) return set_err(AT3R_ERR_INVALID_ARGUMENT, "only SART plans fill empty voxels");
+    const size_t m = (size_t)p->Nx * p->Nz;
+    if (n < m) return set_err(AT3R_ERR_INVALID_ARGUMENT, "table capacity below Nx * Nz entries");
+    int* d = nullptr;
+    AT3R_CUDA(cudaMalloc(&d, sizeof(int) * m));
+    k_fill_table<<<(unsigned)((m + 255) / 256), 256>>>(d, (int)m, p->fill_seed);
+    cudaError_t e = cudaMemcpy(table, d, sizeof(int) * m, cudaMemcpyDeviceToHost);
+    cudaFree(d);
+    if (e != cudaSuccess) return set_err(AT3R_ERR_CUDA, std::string("fill table: ") + cudaGetErrorString(e));
+    return AT3R_OK;
+}
+
 const char* at3r_status_str(at3r_status s)
 {
     switch (s) {
@@ -1228,10 +1280,10 @@ extern "C" {
 // The array is AT3R_NOALLOC_SCRATCH_BYTES (16 MiB) on every GPU the library
 // is loaded on, held until the process exits.  Every call shares it and it
 // keeps the last call's contents, so calls that overlap on the GPU (two
-// streams, two threads) race; serialise them.  The first call on a device
-// looks up the array's device address (and raises the back-projection
-// kernel's shared-memory limit); make that first call before any stream
-// capture.
+// streams, two threads) race; serialise them.  Every call looks up the
+// array's device address; the first call on a device also raises the
+// back-projection kernel's shared-memory limit; make that first call before
+// any stream capture.
 // ===========================================================================
 namespace {
 
@@ -1242,15 +1294,12 @@ constexpr size_t kNoallocHeader = sizeof(float2) * kNoallocMaxTilts + sizeof(int
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoallocBytes];
 
+// The array's device address on the current device.  Looked up on every call
+// (a cheap query), so it stays right if the device's context is rebuilt.  The
+// first call on a device also raises the back-projection kernel's
+// shared-memory limit (once per device and process).
 at3r_status noalloc_scratch_address(unsigned char** out)
 {
-    static std::mutex mu;
-    static std::map<int, unsigned char*> addr;
-    int dev = 0;
-    AT3R_CUDA(cudaGetDevice(&dev));
-    std::lock_guard<std::mutex> lk(mu);
-    auto it = addr.find(dev);
-    if (it != addr.end()) { *out = it->second; return AT3R_OK; }
     void* ptr = nullptr;
     cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
     if (e != cudaSuccess || !ptr) {
@@ -1260,9 +1309,19 @@ at3r_status noalloc_scratch_address(unsigned char** out)
     }
     at3r_status rc = set_smem((const void*)k_bp<0, float, float, false>, 0);
     if (rc != AT3R_OK) return rc;
-    addr[dev] = (unsigned char*)ptr;
     *out = (unsigned char*)ptr;
     return AT3R_OK;
+}
+
+// Writes a chunk of the cos/sin table into the scratch header: the values
+// travel in the launch's parameters, so no host buffer has to outlive the call.
+constexpr int kCsChunk = 448;   // 3.5 KB of parameters per launch
+struct CsChunk {
+    float2 v[kCsChunk];
+};
+__global__ void k_put_cs(CsChunk c, int n, float2* __restrict__ dst)
+{
+    for (int i = threadIdx.x; i < n; i += blockDim.x) dst[i] = c.v[i];
 }
 
 }  // namespace
@@ -1311,7 +1370,13 @@ extern "C" at3r_status at3r_sart_device_noalloc(const float* proj, int nx, int n
     float* d_raw = reinterpret_cast<float*>(base + kNoallocHeader);
     float* d_diff = d_raw + (size_t)slab * T * N;
     cudaStream_t st = (cudaStream_t)stream;
-    AT3R_CUDA(cudaMemcpyAsync(d_cs, cs.data(), sizeof(float) * 2 * T, cudaMemcpyHostToDevice, st));
+    for (int t0 = 0; t0 < T; t0 += kCsChunk) {
+        CsChunk c{};
+        const int n = std::min(kCsChunk, T - t0);
+        for (int i = 0; i < n; i++) c.v[i] = make_float2(cs[2 * (t0 + i)], cs[2 * (t0 + i) + 1]);
+        k_put_cs<<<1, 256, 0, st>>>(c, n, d_cs + t0);
+        AT3R_CUDA(cudaGetLastError());
+    }
 
     // contiguous subsets of [start_tilt, start_tilt + num_tilts), the first n % k one larger
     std::vector<int> sub_start(subsets, 0), sub_size(subsets, num_tilts / subsets);
@@ -1319,6 +1384,9 @@ extern "C" at3r_status at3r_sart_device_noalloc(const float* proj, int nx, int n
     for (int i = 1; i < subsets; i++) sub_start[i] = sub_start[i - 1] + sub_size[i - 1];
     const float rlx = relax > 0.f ? relax : 1.0f / (float)subsets;
     const size_t tilt_stride = (size_t)ny * nx;
+    // the empty-voxel fill's table is drawn per call from the time, as the
+    // reference draws it per series (GGenRandoms::DoIt)
+    const unsigned long long fill_seed = (unsigned long long)time(nullptr);
     for (int y0 = 0; y0 < ny; y0 += slab) {
         const int S = std::min(slab, ny - y0);
         float* v = vol + (size_t)y0 * Nx * Nz;
@@ -1349,7 +1417,10 @@ extern "C" at3r_status at3r_sart_device_noalloc(const float* proj, int nx, int n
                 AT3R_CUDA(cudaGetLastError());
             }
         }
-        k_fill_empty<<<S, 256, 0, st>>>(v, (size_t)Nx * Nz, d_flags);
+        const int fb = std::max(1, std::min((Nx * Nz + 255) / 256, (8 * 148 + S - 1) / S));
+        k_fill_mark<<<dim3(fb, S), 256, 0, st>>>(v, Nx, Nz, d_flags, fill_seed, nullptr);
+        AT3R_CUDA(cudaGetLastError());
+        k_fill_finish<<<S, 512, 0, st>>>(v, Nx, Nz, d_flags, nullptr);
         AT3R_CUDA(cudaGetLastError());
     }
     return AT3R_OK;

@@ -16,11 +16,17 @@
 #include <type_traits>
 
 #include "fft_smem.cuh"
+#include "rand_table.cuh"
 
 namespace at3r {
 
 constexpr float kSentinelTest = -1e10f;   // "empty sample" threshold of the reference
 constexpr float kSentinelValue = -1e30f;  // value the reference writes for "no sample"
+// 16-bit storage keeps the -1e30 "no sample" class as a marker (NaN) instead
+// of a value: every value at or below this (the weighted -1e30 lies far
+// below it) is stored as the marker; every other value keeps its magnitude,
+// so a value between -1e20 and -1e10 still lerps as the reference lerps it.
+constexpr float kStoreMissing = -1e20f;
 
 // floor without the conversion units: for 0 <= x < 2^23, x + 2^23 rounded
 // down is 2^23 + floor(x) exactly, so its bit pattern minus kMagicBits is
@@ -30,8 +36,12 @@ constexpr int kMagicBits = 0x4B000000;
 
 // ---------------------------------------------------------------------------
 // Storage of staged sinograms.  FP32 as is; FP16 / BF16 as value / scale with
-// one scale per (slice, tilt) row (the row's largest magnitude), so a row
-// spans [-1, 1] whatever its level.  Accumulation is always FP32.
+// one scale per (slice, tilt) row (the row's largest magnitude, the -1e30
+// "no sample" markers left out), so a row spans [-1, 1] whatever its level.
+// Accumulation is always FP32.  A row keeps 2^-24 (FP16) or 2^-133 (BF16) of
+// its largest magnitude: FP16 loses the ordinary values of a row that also
+// holds a value ten orders of magnitude larger (as near-threshold test inputs
+// do); BF16 does not.
 // ---------------------------------------------------------------------------
 template <typename ST>
 struct Stor;
@@ -49,7 +59,7 @@ struct Stor<__half> {
     __device__ __forceinline__ static float ld(const __half* p, float scale) { return unscale(__half2float(__ldg(p)), scale); }
     __device__ __forceinline__ static void st(__half* p, float v, float inv)
     {
-        *p = __float2half_rn(v <= kSentinelTest ? __int_as_float(0x7fc00000) : v * inv);
+        *p = __float2half_rn(v <= kStoreMissing ? __int_as_float(0x7fc00000) : v * inv);
     }
 };
 template <>
@@ -60,26 +70,8 @@ struct Stor<__nv_bfloat16> {
     }
     __device__ __forceinline__ static void st(__nv_bfloat16* p, float v, float inv)
     {
-        *p = __float2bfloat16_rn(v <= kSentinelTest ? __int_as_float(0x7fc00000) : v * inv);
+        *p = __float2bfloat16_rn(v <= kStoreMissing ? __int_as_float(0x7fc00000) : v * inv);
     }
-};
-
-// Two slices of the 16-bit volume shadow the forward projector reads.
-template <typename VT>
-struct Pair;
-template <>
-struct Pair<__half> {
-    using T2 = __half2;
-    __device__ __forceinline__ static float2 ld(const __half2* p) { return __half22float2(__ldg(p)); }
-    __device__ __forceinline__ static __half2 make(float a, float b) { return __floats2half2_rn(a, b); }
-    __device__ __forceinline__ static __half one(float a) { return __float2half_rn(a); }
-};
-template <>
-struct Pair<__nv_bfloat16> {
-    using T2 = __nv_bfloat162;
-    __device__ __forceinline__ static float2 ld(const __nv_bfloat162* p) { return __bfloat1622float2(__ldg(p)); }
-    __device__ __forceinline__ static __nv_bfloat162 make(float a, float b) { return __floats2bfloat162_rn(a, b); }
-    __device__ __forceinline__ static __nv_bfloat16 one(float a) { return __float2bfloat16_rn(a); }
 };
 
 // Four slices of the SART working volume at one voxel (the slice-group
@@ -204,7 +196,7 @@ __global__ void __launch_bounds__(256) k_gather_weight(const float* __restrict__
         float m = 0.f;
         for (int x = threadIdx.x; x < N; x += blockDim.x) {
             const float v = __ldg(src + x) * w;
-            if (v > kSentinelTest) m = fmaxf(m, fabsf(v));
+            if (v > kStoreMissing) m = fmaxf(m, fabsf(v));
         }
         const float sc = row_scale(block_absmax(m, red));
         inv = 1.f / sc;
@@ -275,7 +267,7 @@ __global__ void __launch_bounds__(512, RS < 2 ? 2 : 1) k_rweight(const float* __
             for (int x = lane; x < N; x += 32) {
                 const float2 w2 = rq[fft_pad(x)];
                 const float v = c ? w2.y : w2.x;
-                if (v > kSentinelTest) m = fmaxf(m, fabsf(v));
+                if (v > kStoreMissing) m = fmaxf(m, fabsf(v));
             }
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
@@ -351,8 +343,9 @@ struct BpArgs {
     int ww;                  // staged window width (samples)
     int* flags;              // per-slice flag bits
     int low_bit;             // the flag bit that marks this sinogram as holding low values
-    void* shadow;            // MODE 0, 16-bit volume type: [ceil(slices/2)][GZ][GX] slice pairs (z flipped),
-                             // or [groups][GZ][GX] of four 16-bit values beside the slice-group volume
+    void* shadow;            // MODE 0, 16-bit volume type: [ceil(slices/8)][GZ][GX] of eight 16-bit values
+                             // beside the slice-group volume (shadow_half)
+    int* seen;               // run summary: the flags of every slice ORed in (may be null)
 };
 
 template <int MODE>
@@ -398,19 +391,13 @@ __device__ __forceinline__ float bp_store(const BpArgs& p, int ys, int Z, int X,
     }
 }
 
-// The 16-bit shadow of the SART volume: slices (2g, 2g+1) share one word.
-template <typename VT>
-__device__ __forceinline__ void shadow_pair(const BpArgs& p, int ys, int Z, int X, float a, float b)
+// The 16-bit shadow of the SART working volume holds eight slices per voxel
+// ([ceil(S/8)][GZ][GX] x 16 bytes, rows z flipped), so that one forward-
+// projection load gives a tap of eight slices; slice group g (four slices)
+// is the half g & 1 of element g >> 1.  Index of that half, in 8-byte units.
+__device__ __forceinline__ size_t shadow_half(const BpArgs& p, int g, int Z, int X)
 {
-    using T2 = typename Pair<VT>::T2;
-    T2* sh = reinterpret_cast<T2*>(p.shadow) + ((size_t)(ys >> 1) * p.GZ + (p.GZ - 1 - Z)) * p.GX + X;
-    *sh = Pair<VT>::make(a, b);
-}
-template <typename VT>
-__device__ __forceinline__ void shadow_one(const BpArgs& p, int ys, int Z, int X, float a)
-{
-    VT* sh = reinterpret_cast<VT*>(p.shadow) + 2 * (((size_t)(ys >> 1) * p.GZ + (p.GZ - 1 - Z)) * p.GX + X) + (ys & 1);
-    *sh = Pair<VT>::one(a);
+    return 2 * (((size_t)(g >> 1) * p.GZ + (p.GZ - 1 - Z)) * p.GX + X) + (g & 1);
 }
 
 // SART update of one voxel of the slice-group working volume
@@ -447,7 +434,8 @@ __device__ __forceinline__ void bp_store_grp(const BpArgs& p, int g, int ys0, in
         for (int q = 0; q < 4; q++)
             if ((empty >> q) & 1) atomicOr(p.flags + ys0 + q, kFlagVolEmpty);
     }
-    if constexpr (!std::is_same<VT, float>::value) reinterpret_cast<uint2*>(p.shadow)[idx] = Quad<VT>::make(nv);
+    if constexpr (!std::is_same<VT, float>::value) reinterpret_cast<uint2*>(p.shadow)[shadow_half(p, g, Z, X)] =
+        Quad<VT>::make(nv);
 }
 template <typename VT>
 __device__ __forceinline__ void bp_store1_grp(const BpArgs& p, int g, int q, int ys, int Z, int X, float sum, int cnt)
@@ -464,7 +452,8 @@ __device__ __forceinline__ void bp_store1_grp(const BpArgs& p, int g, int q, int
         atomicOr(p.flags + ys, kFlagVolEmpty);
     }
     *v = r;
-    if constexpr (!std::is_same<VT, float>::value) Quad<VT>::st1(reinterpret_cast<uint2*>(p.shadow) + idx, q, r);
+    if constexpr (!std::is_same<VT, float>::value)
+        Quad<VT>::st1(reinterpret_cast<uint2*>(p.shadow) + shadow_half(p, g, Z, X), q, r);
 }
 
 // GRP (MODE 0 only): the volume is the slice-group working volume above;
@@ -473,6 +462,7 @@ template <int MODE, typename ST, typename VT, bool GRP>
 __global__ void __launch_bounds__(BP_THREADS, 3) k_bp(BpArgs p)
 {
     static_assert(!GRP || MODE == 0, "the slice-group layout is the SART working volume");
+    static_assert(GRP || std::is_same<VT, float>::value, "the 16-bit shadow exists in the slice-group layout only");
     extern __shared__ float2 bsm[];
     float2* cs_s = bsm;                                               // [BP_CHUNK]
     float2* pw = bsm + BP_CHUNK;                                      // [SB][BP_CHUNK][BP_WW]
@@ -487,6 +477,8 @@ __global__ void __launch_bounds__(BP_THREADS, 3) k_bp(BpArgs p)
 
     bool low = false;
     for (int q = 0; q < nsl; q++) low |= (__ldg(p.flags + ys0 + q) & p.low_bit) != 0;
+    if (p.seen && blockIdx.x == 0 && blockIdx.y == 0 && (int)threadIdx.x < nsl)
+        atomicOr(p.seen, __ldg(p.flags + ys0 + threadIdx.x));
 
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     float fX[BP_CX], fZ[BP_CZ];
@@ -643,16 +635,10 @@ __global__ void __launch_bounds__(BP_THREADS, 3) k_bp(BpArgs p)
                     bp_store_grp<VT>(p, blockIdx.z, ys0, nsl, Z, X,
                                      make_float4(sum[0][j][i], sum[1][j][i], sum[2][j][i], sum[3][j][i]), cnt[j][i]);
                 } else {
-                    float nv[SB];
                     const float k = cnt[j][i] > 0 ? __fdiv_rn(MODE == 0 ? p.relax : 1.f, (float)cnt[j][i]) : 0.f;
 #pragma unroll
                     for (int q = 0; q < SB; q++)
-                        nv[q] = q < nsl ? bp_store<MODE>(p, ys0 + q, Z, X, sum[q][j][i], cnt[j][i], k) : 0.f;
-                    if constexpr (MODE == 0 && !std::is_same<VT, float>::value) {
-#pragma unroll
-                        for (int g = 0; g < SB / 2; g++)
-                            if (2 * g < nsl) shadow_pair<VT>(p, ys0 + 2 * g, Z, X, nv[2 * g], nv[2 * g + 1]);
-                    }
+                        if (q < nsl) bp_store<MODE>(p, ys0 + q, Z, X, sum[q][j][i], cnt[j][i], k);
                 }
             }
         }
@@ -684,7 +670,8 @@ __global__ void __launch_bounds__(BP_THREADS, 3) k_bp(BpArgs p)
                         const float fr = __fsub_rn(xp, (float)ii);
                         const float2 v2 = w[min((unsigned)(ii - st), wmax)];
                         const float v = __fmaf_rn(v2.x, __fsub_rn(1.f, fr), __fmul_rn(v2.y, fr));
-                        if (xp >= 0.f && xp <= endX && v > kSentinelTest) {
+                        // the reference skips v <= -1e10 (a NaN sample is summed)
+                        if (xp >= 0.f && xp <= endX && !(v <= kSentinelTest)) {
                             sum[j][i] = __fadd_rn(sum[j][i], v);
                             cnt[j][i] += 1;
                         }
@@ -704,8 +691,7 @@ __global__ void __launch_bounds__(BP_THREADS, 3) k_bp(BpArgs p)
                         bp_store1_grp<VT>(p, blockIdx.z, q, ys0 + q, Z, X, sum[j][i], cnt[j][i]);
                     } else {
                         const float k = cnt[j][i] > 0 ? __fdiv_rn(MODE == 0 ? p.relax : 1.f, (float)cnt[j][i]) : 0.f;
-                        const float nv = bp_store<MODE>(p, ys0 + q, Z, X, sum[j][i], cnt[j][i], k);
-                        if constexpr (MODE == 0 && !std::is_same<VT, float>::value) shadow_one<VT>(p, ys0 + q, Z, X, nv);
+                        bp_store<MODE>(p, ys0 + q, Z, X, sum[j][i], cnt[j][i], k);
                     }
                 }
             }
@@ -786,12 +772,26 @@ __device__ __forceinline__ float bilerp(float a00, float a10, float a01, float a
     return __fmaf_rn(wx, B - A, A);
 }
 
+// Slices one forward-projection thread carries: four of the FP32 volume (one
+// float4 tap); eight of the 16-bit shadow (one 16-byte tap), which halves the
+// per-slice cost of the sample positions, weights and loads.
+template <typename VT>
+__host__ __device__ constexpr int fp_slices()
+{
+    return std::is_same<VT, float>::value ? 4 : 8;
+}
+
+// bf16 pair -> two floats: a bf16 is the upper half of an FP32 word.
+__device__ __forceinline__ float bf_lo(uint32_t u) { return __uint_as_float(u << 16); }
+__device__ __forceinline__ float bf_hi(uint32_t u) { return __uint_as_float(u & 0xffff0000u); }
+
 // ST: storage of raw / diff rows; VT: float reads the FP32 volume, __half /
 // __nv_bfloat16 read its 16-bit shadow — the FP32 volume is then read only
-// for slices that may hold "empty" voxels.  GRP: the volume (and shadow) are
-// in the slice-group layout, so one load gives a tap of all four slices;
-// otherwise the volume is plain [slices][Nz][Nx] and the shadow holds slice
-// pairs.
+// for slices that may hold "empty" voxels.  GRP: the volume is in the
+// slice-group layout (one float4 load gives a tap of four slices) and the
+// shadow holds eight slices per voxel (one 16-byte load gives a tap of
+// eight); otherwise (FP32 only) the volume is plain [slices][Nz][Nx].
+// Grid (ceil(N/256), tilts, ceil(slices / fp_slices<VT>())).
 template <typename ST, typename VT, bool GRP>
 __global__ void __launch_bounds__(256) k_fp_diff(const float* __restrict__ vol, const void* __restrict__ shadow,
                                                  int Nx, int Nz, int S, const ST* __restrict__ raw,
@@ -799,8 +799,10 @@ __global__ void __launch_bounds__(256) k_fp_diff(const float* __restrict__ vol, 
                                                  const float2* __restrict__ cs, int T, int N, int t0,
                                                  double* __restrict__ rf, int* __restrict__ flags)
 {
+    static_assert(GRP || std::is_same<VT, float>::value, "the 16-bit shadow exists in the slice-group layout only");
+    constexpr int NS = fp_slices<VT>();
     const int u = blockIdx.x * blockDim.x + threadIdx.x;
-    const int t = t0 + blockIdx.y, ys0 = blockIdx.z * SB, nsl = min(SB, S - ys0);
+    const int t = t0 + blockIdx.y, ys0 = blockIdx.z * NS, nsl = min(NS, S - ys0);
     const bool active = u < N;
     const float2 cc = __ldg(&cs[t]);
     RayPos r;
@@ -815,106 +817,87 @@ __global__ void __launch_bounds__(256) k_fp_diff(const float* __restrict__ vol, 
     bool empty_vox = false;
     for (int q = 0; q < nsl; q++) empty_vox |= (__ldg(flags + ys0 + q) & kFlagVolEmpty) != 0;
 
-    float fSum[SB], fCount[SB];
+    float fSum[NS], fCount[NS];
 #pragma unroll
-    for (int q = 0; q < SB; q++) { fSum[q] = 0.f; fCount[q] = 0.f; }
-    bool shadow_done = false;
-    if constexpr (GRP) {
-      if (!empty_vox) {
-        shadow_done = true;
-        // slice group: one load per tap; rows of voxel Z and Z + 1 as bases
-        using T4 = typename Quad<VT>::T4;
-        const T4* g0 = (std::is_same<VT, float>::value ? reinterpret_cast<const T4*>(vol)
-                                                        : reinterpret_cast<const T4*>(shadow)) +
-                       (size_t)blockIdx.z * slice + (size_t)(Nz - 1) * Nx;
-        const T4* g1 = g0 - Nx;
+    for (int q = 0; q < NS; q++) { fSum[q] = 0.f; fCount[q] = 0.f; }
+    if (GRP && !empty_vox) {
         // cell offset iX - iZ*Nx from the bits of x + 2^23 and z + 2^23
         // (wrapping 32-bit arithmetic; the true value fits an int)
         const unsigned kx = (unsigned)kMagicBits * (unsigned)(Nx - 1);
         float fi = (float)wlo;   // i as a float, exact below 2^24
-        for (int i = wlo; i <= whi; i++, fi += 1.f) {
-            if (i < lo || i > hi) continue;
-            const float fd = fi - r.halfL;   // exact: the sample index of RayPos
-            const float fX = __fmaf_rn(-fd, r.s, r.tx), fZ = __fmaf_rn(fd, r.c, r.tz);
-            const float tX = __fadd_rd(fX, kMagic), tZ = __fadd_rd(fZ, kMagic);
-            const float wx = fX - (tX - kMagic), wz = fZ - (tZ - kMagic);
-            const int o = (int)((unsigned)__float_as_int(tX) - (unsigned)__float_as_int(tZ) * (unsigned)Nx + kx);
-            const float ux = 1.f - wx, uz = 1.f - wz;
-            const float w00 = ux * uz, w10 = wx * uz, w01 = ux * wz, w11 = wx * wz;
-            if constexpr (std::is_same<VT, __half>::value) {
-                // FP16 shadow: the sample value of two slices per half2
-                // instruction, added to the FP32 sums by mixed-precision adds
-                const uint2 b00 = __ldg(reinterpret_cast<const uint2*>(g0 + o));
-                const uint2 b10 = __ldg(reinterpret_cast<const uint2*>(g0 + o + 1));
-                const uint2 b01 = __ldg(reinterpret_cast<const uint2*>(g1 + o));
-                const uint2 b11 = __ldg(reinterpret_cast<const uint2*>(g1 + o + 1));
-                const __half2 h00 = __float2half2_rn(w00), h10 = __float2half2_rn(w10);
-                const __half2 h01 = __float2half2_rn(w01), h11 = __float2half2_rn(w11);
-                __half2 lo = __hmul2(h00, from_bits<__half2>(b00.x));
-                __half2 hi = __hmul2(h00, from_bits<__half2>(b00.y));
-                lo = __hfma2(h10, from_bits<__half2>(b10.x), lo);
-                hi = __hfma2(h10, from_bits<__half2>(b10.y), hi);
-                lo = __hfma2(h01, from_bits<__half2>(b01.x), lo);
-                hi = __hfma2(h01, from_bits<__half2>(b01.y), hi);
-                lo = __hfma2(h11, from_bits<__half2>(b11.x), lo);
-                hi = __hfma2(h11, from_bits<__half2>(b11.y), hi);
-                fSum[0] = add_f32_f16(fSum[0], __low2half(lo));
-                fSum[1] = add_f32_f16(fSum[1], __high2half(lo));
-                fSum[2] = add_f32_f16(fSum[2], __low2half(hi));
-                fSum[3] = add_f32_f16(fSum[3], __high2half(hi));
-                continue;
+        if constexpr (std::is_same<VT, float>::value) {
+            // slice group: one float4 load per tap; rows of voxel Z and Z + 1 as bases
+            const float4* g0 = reinterpret_cast<const float4*>(vol) + (size_t)blockIdx.z * slice + (size_t)(Nz - 1) * Nx;
+            const float4* g1 = g0 - Nx;
+            for (int i = wlo; i <= whi; i++, fi += 1.f) {
+                if (i < lo || i > hi) continue;
+                const float fd = fi - r.halfL;   // exact: the sample index of RayPos
+                const float fX = __fmaf_rn(-fd, r.s, r.tx), fZ = __fmaf_rn(fd, r.c, r.tz);
+                const float tX = __fadd_rd(fX, kMagic), tZ = __fadd_rd(fZ, kMagic);
+                const float wx = fX - (tX - kMagic), wz = fZ - (tZ - kMagic);
+                const int o = (int)((unsigned)__float_as_int(tX) - (unsigned)__float_as_int(tZ) * (unsigned)Nx + kx);
+                const float ux = 1.f - wx, uz = 1.f - wz;
+                const float w00 = ux * uz, w10 = wx * uz, w01 = ux * wz, w11 = wx * wz;
+                const float4 a00 = __ldg(g0 + o), a10 = __ldg(g0 + o + 1);
+                const float4 a01 = __ldg(g1 + o), a11 = __ldg(g1 + o + 1);
+                fSum[0] = __fmaf_rn(w11, a11.x, __fmaf_rn(w01, a01.x, __fmaf_rn(w10, a10.x, __fmaf_rn(w00, a00.x, fSum[0]))));
+                fSum[1] = __fmaf_rn(w11, a11.y, __fmaf_rn(w01, a01.y, __fmaf_rn(w10, a10.y, __fmaf_rn(w00, a00.y, fSum[1]))));
+                fSum[2] = __fmaf_rn(w11, a11.z, __fmaf_rn(w01, a01.z, __fmaf_rn(w10, a10.z, __fmaf_rn(w00, a00.z, fSum[2]))));
+                fSum[3] = __fmaf_rn(w11, a11.w, __fmaf_rn(w01, a01.w, __fmaf_rn(w10, a10.w, __fmaf_rn(w00, a00.w, fSum[3]))));
             }
-            const float4 a00 = Quad<VT>::ld(g0 + o), a10 = Quad<VT>::ld(g0 + o + 1);
-            const float4 a01 = Quad<VT>::ld(g1 + o), a11 = Quad<VT>::ld(g1 + o + 1);
-            fSum[0] = __fmaf_rn(w11, a11.x, __fmaf_rn(w01, a01.x, __fmaf_rn(w10, a10.x, __fmaf_rn(w00, a00.x, fSum[0]))));
-            fSum[1] = __fmaf_rn(w11, a11.y, __fmaf_rn(w01, a01.y, __fmaf_rn(w10, a10.y, __fmaf_rn(w00, a00.y, fSum[1]))));
-            fSum[2] = __fmaf_rn(w11, a11.z, __fmaf_rn(w01, a01.z, __fmaf_rn(w10, a10.z, __fmaf_rn(w00, a00.z, fSum[2]))));
-            fSum[3] = __fmaf_rn(w11, a11.w, __fmaf_rn(w01, a01.w, __fmaf_rn(w10, a10.w, __fmaf_rn(w00, a00.w, fSum[3]))));
-        }
-        const float n = (float)max(hi - lo + 1, 0);
+        } else {
+            // 16-bit shadow, eight slices per 16-byte tap
+            const uint4* g0 = reinterpret_cast<const uint4*>(shadow) + (size_t)blockIdx.z * slice + (size_t)(Nz - 1) * Nx;
+            const uint4* g1 = g0 - Nx;
+            for (int i = wlo; i <= whi; i++, fi += 1.f) {
+                if (i < lo || i > hi) continue;
+                const float fd = fi - r.halfL;
+                const float fX = __fmaf_rn(-fd, r.s, r.tx), fZ = __fmaf_rn(fd, r.c, r.tz);
+                const float tX = __fadd_rd(fX, kMagic), tZ = __fadd_rd(fZ, kMagic);
+                const float wx = fX - (tX - kMagic), wz = fZ - (tZ - kMagic);
+                const int o = (int)((unsigned)__float_as_int(tX) - (unsigned)__float_as_int(tZ) * (unsigned)Nx + kx);
+                const float ux = 1.f - wx, uz = 1.f - wz;
+                const float w00 = ux * uz, w10 = wx * uz, w01 = ux * wz, w11 = wx * wz;
+                const uint4 b00 = __ldg(g0 + o), b10 = __ldg(g0 + o + 1);
+                const uint4 b01 = __ldg(g1 + o), b11 = __ldg(g1 + o + 1);
+                const uint32_t p00[4] = {b00.x, b00.y, b00.z, b00.w}, p10[4] = {b10.x, b10.y, b10.z, b10.w};
+                const uint32_t p01[4] = {b01.x, b01.y, b01.z, b01.w}, p11[4] = {b11.x, b11.y, b11.z, b11.w};
+                if constexpr (std::is_same<VT, __half>::value) {
+                    // the sample value of two slices per half2 instruction,
+                    // added to the FP32 sums by mixed-precision adds
+                    const __half2 h00 = __float2half2_rn(w00), h10 = __float2half2_rn(w10);
+                    const __half2 h01 = __float2half2_rn(w01), h11 = __float2half2_rn(w11);
 #pragma unroll
-        for (int q = 0; q < SB; q++) fCount[q] = n;
-      }
-    } else if constexpr (!std::is_same<VT, float>::value) {
-      if (!empty_vox) {
-        shadow_done = true;
-        using T2 = typename Pair<VT>::T2;
-        // two slice pairs; rows of voxel Z and Z + 1 as loop-invariant bases
-        const T2* sbase = reinterpret_cast<const T2*>(shadow) + (size_t)(Nz - 1) * Nx;
-        const T2* r0[SB / 2];
-        const T2* r1[SB / 2];
+                    for (int k = 0; k < 4; k++) {
+                        __half2 v = __hmul2(h00, from_bits<__half2>(p00[k]));
+                        v = __hfma2(h10, from_bits<__half2>(p10[k]), v);
+                        v = __hfma2(h01, from_bits<__half2>(p01[k]), v);
+                        v = __hfma2(h11, from_bits<__half2>(p11[k]), v);
+                        fSum[2 * k] = add_f32_f16(fSum[2 * k], __low2half(v));
+                        fSum[2 * k + 1] = add_f32_f16(fSum[2 * k + 1], __high2half(v));
+                    }
+                } else {
 #pragma unroll
-        for (int g = 0; g < SB / 2; g++) {
-            r0[g] = sbase + (size_t)((ys0 >> 1) + g) * slice;
-            r1[g] = r0[g] - Nx;
-        }
-        for (int i = wlo; i <= whi; i++) {
-            if (i < lo || i > hi) continue;
-            const float fX = r.x(i), fZ = r.z(i);
-            const int iX = (int)fX, iZ = (int)fZ;
-            const float wx = fX - (float)iX, wz = fZ - (float)iZ;
-            const int o = iX - iZ * Nx;
-#pragma unroll
-            for (int g = 0; g < SB / 2; g++) {
-                const float2 a00 = Pair<VT>::ld(r0[g] + o), a10 = Pair<VT>::ld(r0[g] + o + 1);
-                const float2 a01 = Pair<VT>::ld(r1[g] + o), a11 = Pair<VT>::ld(r1[g] + o + 1);
-                fSum[2 * g] += bilerp(a00.x, a10.x, a01.x, a11.x, wx, wz);
-                fSum[2 * g + 1] += bilerp(a00.y, a10.y, a01.y, a11.y, wx, wz);
+                    for (int k = 0; k < 4; k++) {
+                        fSum[2 * k] = __fmaf_rn(w11, bf_lo(p11[k]), __fmaf_rn(w01, bf_lo(p01[k]),
+                                      __fmaf_rn(w10, bf_lo(p10[k]), __fmaf_rn(w00, bf_lo(p00[k]), fSum[2 * k]))));
+                        fSum[2 * k + 1] = __fmaf_rn(w11, bf_hi(p11[k]), __fmaf_rn(w01, bf_hi(p01[k]),
+                                          __fmaf_rn(w10, bf_hi(p10[k]), __fmaf_rn(w00, bf_hi(p00[k]), fSum[2 * k + 1]))));
+                    }
+                }
             }
         }
         const float n = (float)max(hi - lo + 1, 0);
 #pragma unroll
-        for (int q = 0; q < SB; q++) fCount[q] = n;
-      }
-    }
-    if (shadow_done) {
+        for (int q = 0; q < NS; q++) fCount[q] = n;
     } else if (!empty_vox) {
-        // per slice, the rows of voxel Z and Z + 1 as loop-invariant bases; a
-        // sample then costs one 32-bit cell offset and one wide add per row
-        const float* r0[SB];
-        const float* r1[SB];
+        // plain layout (FP32): per slice, the rows of voxel Z and Z + 1 as
+        // loop-invariant bases; a sample then costs one 32-bit cell offset
+        // and one wide add per row
+        const float* r0[NS];
+        const float* r1[NS];
 #pragma unroll
-        for (int q = 0; q < SB; q++) {
+        for (int q = 0; q < NS; q++) {
             r0[q] = vbase + (size_t)(ys0 + min(q, nsl - 1)) * slice;
             r1[q] = r0[q] - Nx;
         }
@@ -925,7 +908,7 @@ __global__ void __launch_bounds__(256) k_fp_diff(const float* __restrict__ vol, 
             const float wx = fX - (float)iX, wz = fZ - (float)iZ;
             const int o = iX - iZ * Nx;   // within one slice: |o| < Nx * Nz
 #pragma unroll
-            for (int q = 0; q < SB; q++) {
+            for (int q = 0; q < NS; q++) {
                 const float* p0 = r0[q] + o;
                 const float* p1 = r1[q] + o;
                 fSum[q] += bilerp(__ldg(p0), __ldg(p0 + 1), __ldg(p1), __ldg(p1 + 1), wx, wz);
@@ -933,13 +916,16 @@ __global__ void __launch_bounds__(256) k_fp_diff(const float* __restrict__ vol, 
         }
         const float n = (float)max(hi - lo + 1, 0);
 #pragma unroll
-        for (int q = 0; q < SB; q++) fCount[q] = n;
+        for (int q = 0; q < NS; q++) fCount[q] = n;
     } else {
-        // element stride: 4 in the slice-group layout, 1 in the plain one
+        // slices that may hold empty voxels: one at a time from the FP32
+        // volume (slice-group layout: group (ys0+q)/4, component (ys0+q)%4)
+        // with the reference's per-sample test
         constexpr int E = GRP ? 4 : 1;
         for (int q = 0; q < nsl; q++) {
-            const float* v0 = GRP ? vol + E * ((size_t)blockIdx.z * slice + (size_t)(Nz - 1) * Nx) + q
-                                  : vbase + (size_t)(ys0 + q) * slice;
+            const int ys = ys0 + q;
+            const float* v0 = GRP ? vol + E * ((size_t)(ys >> 2) * slice + (size_t)(Nz - 1) * Nx) + (ys & 3)
+                                  : vbase + (size_t)ys * slice;
             float s0 = 0.f, n0 = 0.f;
             for (int i = wlo; i <= whi; i++) {
                 if (i < lo || i > hi) continue;
@@ -953,7 +939,7 @@ __global__ void __launch_bounds__(256) k_fp_diff(const float* __restrict__ vol, 
                 n0 += 1.f;
             }
 #pragma unroll
-            for (int k = 0; k < SB; k++)
+            for (int k = 0; k < NS; k++)
                 if (k == q) { fSum[k] = s0; fCount[k] = n0; }
         }
     }
@@ -961,7 +947,7 @@ __global__ void __launch_bounds__(256) k_fp_diff(const float* __restrict__ vol, 
     float ad = 0.f, ar = 0.f;
     if (active) {
 #pragma unroll
-        for (int q = 0; q < SB; q++) {
+        for (int q = 0; q < NS; q++) {
             if (q >= nsl) continue;
             const float fp = fCount[q] <= 0.f ? kSentinelValue : fSum[q] / fCount[q];
             const size_t row = (size_t)(ys0 + q) * T + t;
@@ -1035,32 +1021,108 @@ __global__ void __launch_bounds__(256) k_flip_rows(const float* __restrict__ in,
 }
 
 // ---------------------------------------------------------------------------
-// Replace any "-1e30" voxel of a flagged slice (MaUtil/GFillEmpty2D.cu runs
-// after SART, AreTomo/Recon/CTomoSart.cpp:88).  The reference copies a
-// time-seeded random valid voxel; this fills the slice's valid mean, which is
-// deterministic.  From a zero start no voxel reaches the sentinel unless the
-// input holds values near -1e10, so this is a guard.  Grid (slices).
+// Empty-voxel fill after SART (AreTomo/Recon/CTomoSart.cpp:88 ->
+// MaUtil/GFillEmpty2D.cu:7-143, table of MaUtil/GGenRandoms.cu): on every
+// slice with empty voxels (value below -1e10, flag bit), an empty voxel
+// follows its chain through the random table — at most 100 links — to the
+// first non-empty voxel and takes its value; a chain that finds none takes the
+// mean of the slice's non-empty voxels, summed as the reference's single
+// 512-thread block sums it.  Voxel indices are the reference's, i = Z*Nx + X
+// in its unflipped slice; here voxel (X, Z) lives in row Nz-1-Z of
+// vol[S][Nz][Nx].  Table entries are drawn on the fly (rand_table.cuh), so no
+// table is stored.
+//
+// Two passes, in place.  k_fill_mark: each empty voxel finds its source and
+// is overwritten with a marker, a float below -1e10 whose bits encode the
+// source index (kFillMark + k) or the mean (kFillMarkMean); markers still
+// read as empty, so chains walked at the same time see the state before the
+// fill, as the reference's separate emptiness pass gives them.
+// k_fill_finish: the mean of the non-empty voxels (markers excluded), then
+// every marker is replaced by its source voxel's value (never a marker) or
+// the mean.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) k_fill_empty(float* __restrict__ vol, size_t slice_elems,
-                                                    const int* __restrict__ flags)
+constexpr unsigned kFillMark = 0xD0200000u;       // -1.07e10: marker of source 0
+constexpr unsigned kFillMarkMean = 0xF0200000u;   // -1.98e29: beyond every source (< 2^29 voxels)
+constexpr int kFlagFillMean = 8;                  // a chain found no non-empty voxel (run summary bit)
+
+__device__ __forceinline__ size_t fill_addr(int i, int Nx, int Nz)
 {
-    const int ys = blockIdx.x;
+    const int Z = i / Nx;
+    return (size_t)(Nz - 1 - Z) * Nx + (i - Z * Nx);
+}
+
+// Grid (blocks, S), 256 threads; blocks stride over the slice.
+__global__ void __launch_bounds__(256) k_fill_mark(float* __restrict__ vol, int Nx, int Nz,
+                                                   const int* __restrict__ flags, unsigned long long seed,
+                                                   int* __restrict__ seen)
+{
+    const int ys = blockIdx.y;
     if ((flags[ys] & kFlagVolEmpty) == 0) return;
-    float* v = vol + (size_t)ys * slice_elems;
-    float s = 0.f, n = 0.f;
-    for (size_t i = threadIdx.x; i < slice_elems; i += blockDim.x)
-        if (!(v[i] < kSentinelTest)) { s += v[i]; n += 1.f; }
-    __shared__ float rs[256], rn[256];
-    rs[threadIdx.x] = s;
-    rn[threadIdx.x] = n;
+    const int n = Nx * Nz;
+    float* v = vol + (size_t)ys * n;
+    bool mean_used = false;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const size_t a = fill_addr(i, Nx, Nz);
+        if (!(v[a] < kSentinelTest)) continue;
+        int next = rand_table_entry(seed, i, n);
+        unsigned mark = kFillMarkMean;
+        for (int j = 0; j < 100; j++) {
+            if (v[fill_addr(next, Nx, Nz)] < kSentinelTest) {
+                next = rand_table_entry(seed, next, n);
+                continue;
+            }
+            mark = kFillMark + (unsigned)next;
+            break;
+        }
+        mean_used |= mark == kFillMarkMean;
+        v[a] = __uint_as_float(mark);
+    }
+    if (mean_used && seen) atomicOr(seen, kFlagFillMean);
+}
+
+// Grid S, 512 threads (the reference's mean is one 512-thread block's sum).
+// Also ORs every slice's flags into the run summary `seen` (may be null).
+__global__ void __launch_bounds__(512) k_fill_finish(float* __restrict__ vol, int Nx, int Nz,
+                                                     const int* __restrict__ flags, int* __restrict__ seen)
+{
+    const int ys = blockIdx.x, tid = threadIdx.x;
+    const int f = flags[ys];
+    if (tid == 0 && seen) atomicOr(seen, f);
+    if ((f & kFlagVolEmpty) == 0) return;
+    const int n = Nx * Nz;
+    float* v = vol + (size_t)ys * n;
+    __shared__ float s_sum[512], s_cnt[512];
+    float sum = 0.f, cnt = 0.f;
+    for (int i = tid; i < n; i += 512) {
+        const float x = v[fill_addr(i, Nx, Nz)];
+        if (x < kSentinelTest) continue;
+        sum = __fadd_rn(sum, x);
+        cnt = __fadd_rn(cnt, 1.0f);
+    }
+    s_sum[tid] = sum;
+    s_cnt[tid] = cnt;
     __syncthreads();
-    for (int o = 128; o > 0; o >>= 1) {
-        if ((int)threadIdx.x < o) { rs[threadIdx.x] += rs[threadIdx.x + o]; rn[threadIdx.x] += rn[threadIdx.x + o]; }
+    for (int off = 256; off > 0; off >>= 1) {
+        if (tid < off) {
+            s_sum[tid] = __fadd_rn(s_sum[tid], s_sum[tid + off]);
+            s_cnt[tid] = __fadd_rn(s_cnt[tid], s_cnt[tid + off]);
+        }
         __syncthreads();
     }
-    const float mean = rn[0] > 0.f ? rs[0] / rn[0] : 0.f;
-    for (size_t i = threadIdx.x; i < slice_elems; i += blockDim.x)
-        if (v[i] < kSentinelTest) v[i] = mean;
+    const float mean = s_cnt[0] <= 0.f ? 0.f : __fdiv_rn(s_sum[0], s_cnt[0]);
+    for (int i = tid; i < n; i += 512) {
+        const size_t a = fill_addr(i, Nx, Nz);
+        const unsigned u = __float_as_uint(v[a]);
+        if (u < kFillMark || u > kFillMarkMean) continue;
+        v[a] = u == kFillMarkMean ? mean : v[fill_addr((int)(u - kFillMark), Nx, Nz)];
+    }
+}
+
+// The fill's random table itself, for introspection (the oracle is driven by it).
+__global__ void k_fill_table(int* __restrict__ r, int n, unsigned long long seed)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) r[i] = rand_table_entry(seed, i, n);
 }
 
 // ---------------------------------------------------------------------------

@@ -22,20 +22,15 @@
 #include <stdint.h>
 
 #include "fft_smem.cuh"
+#include "rand_table.cuh"
 
 namespace at3r {
 
-// Random table of the fill, MaUtil/GGenRandoms.cu:7-20: entry i is drawn from
-// subsequence i of the seeded XORWOW generator, scaled to [0, n).
+// Random table of the fill, MaUtil/GGenRandoms.cu:7-20 (rand_table.cuh).
 __global__ void k_rand_table(int* __restrict__ r, int n, unsigned long long seed)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    curandState_t st;
-    curand_init(seed, i, 0, &st);
-    const float u = curand_uniform(&st);
-    const int v = (int)(u * n + 0.5f);
-    r[i] = v % n;
+    if (i < n) r[i] = rand_table_entry(seed, i, n);
 }
 
 // cos / sin of every tilt's rotation (radians), as GCorrPatchShift.cu:77-78

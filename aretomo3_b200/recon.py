@@ -46,6 +46,7 @@ class Geom(ctypes.Structure):
         ("c2r", ctypes.c_int),
         ("slab_slices", ctypes.c_int),
         ("compute_rfactor", ctypes.c_int),
+        ("fill_seed", ctypes.c_ulonglong),
     ]
 
 
@@ -125,6 +126,8 @@ _EXPORTS = {
                                            ctypes.c_int, ctypes.POINTER(ThicknessResult), ctypes.c_void_p]),
     "at3r_mrc_write": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(ctypes.c_void_p), ctypes.c_int, ctypes.c_int,
                                       ctypes.c_int, ctypes.c_float]),
+    "at3r_plan_flags_seen": (ctypes.c_int, [ctypes.c_void_p]),
+    "at3r_plan_fill_table": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t]),
     "at3r_status_str": (ctypes.c_char_p, [ctypes.c_int]),
     "at3r_last_error": (ctypes.c_char_p, []),
 }
@@ -148,9 +151,12 @@ def _check(rc: int) -> None:
 
 
 def make_geom(nx, ny, tilts_deg, vol_z, method=WBP, start_tilt=0, num_tilts=None, iterations=0, subsets=1,
-              relax=0.0, storage=STORE_F32, c2r=C2R_MATCH_CUFFT, slab_slices=0, compute_rfactor=False):
+              relax=0.0, storage=STORE_F32, c2r=C2R_MATCH_CUFFT, slab_slices=0, compute_rfactor=False,
+              fill_seed=None):
     """Fills an at3r_geom; returns it with the tilt array it points into
-    (which the caller keeps alive as long as the struct)."""
+    (which the caller keeps alive as long as the struct).  fill_seed: seed of
+    SART's empty-voxel fill table; None keeps at3r_geom_init's time(0), as the
+    reference seeds it."""
     tilts = np.ascontiguousarray(np.asarray(tilts_deg, dtype=np.float32))
     g = Geom()
     lib().at3r_geom_init(ctypes.byref(g), method)
@@ -162,6 +168,8 @@ def make_geom(nx, ny, tilts_deg, vol_z, method=WBP, start_tilt=0, num_tilts=None
     g.iterations, g.subsets, g.relax = int(iterations), int(subsets), float(relax)
     g.storage, g.c2r, g.slab_slices = int(storage), int(c2r), int(slab_slices)
     g.compute_rfactor = int(bool(compute_rfactor))
+    if fill_seed is not None:
+        g.fill_seed = int(fill_seed)
     return g, tilts
 
 
@@ -170,10 +178,10 @@ class Plan:
 
     def __init__(self, nx, ny, tilts_deg, vol_z, method=WBP, start_tilt=0, num_tilts=None, iterations=0,
                  subsets=1, relax=0.0, storage=STORE_F32, c2r=C2R_MATCH_CUFFT, slab_slices=0,
-                 compute_rfactor=False):
+                 compute_rfactor=False, fill_seed=None):
         L = lib()
         g, self._tilts = make_geom(nx, ny, tilts_deg, vol_z, method, start_tilt, num_tilts, iterations, subsets,
-                                   relax, storage, c2r, slab_slices, compute_rfactor)
+                                   relax, storage, c2r, slab_slices, compute_rfactor, fill_seed)
         self.geom = g
         self.method = method
         self.iterations = int(iterations)
@@ -241,6 +249,21 @@ class Plan:
     @property
     def c2r(self) -> int:
         return int(lib().at3r_plan_c2r(self._h))
+
+    def flags_seen(self) -> int:
+        """Bits of what the last run met (at3r_plan_flags_seen): 1 empty SART
+        voxels (filled), 2 staged projections near the missing-value test, 4
+        the residual near it, 8 a fill chain took the slice mean."""
+        v = int(lib().at3r_plan_flags_seen(self._h))
+        if v < 0:
+            _check(2)
+        return v
+
+    def fill_table(self) -> np.ndarray:
+        """The SART fill's random table, Nx * vol_z int32 (reference voxel order)."""
+        out = np.empty(self.Nx * self.vol_z, np.int32)
+        _check(lib().at3r_plan_fill_table(self._h, out.ctypes.data_as(ctypes.c_void_p), out.size))
+        return out
 
     def autotune(self, proj_ptr: int, vol_ptr: int, stream: int = 0) -> int:
         """Times candidate slab sizes on the given device buffers (overwritten)

@@ -56,9 +56,11 @@ typedef enum at3r_storage { AT3R_STORE_F32 = 0, AT3R_STORE_F16 = 1, AT3R_STORE_B
  * not Hermitian there).  cuFFT, which the reference calls, picks per size:
  * most sizes drop them (HERMITIAN); some (e.g. 1200 x 4096) use a
  * half-length packing algorithm that folds them into even/odd samples
- * (PACKED).  MATCH_CUFFT asks the system cuFFT once per size which it does,
- * so the output equals the reference's; it falls back to HERMITIAN when
- * libcufft cannot be loaded. */
+ * (PACKED).  MATCH_CUFFT asks the system cuFFT once per size and process
+ * which it does (one tiny C2R on a stream of the library's own, with
+ * stream-ordered memory), so the output equals the reference's; when
+ * libcufft cannot be loaded, plan creation fails with AT3R_ERR_UNSUPPORTED
+ * rather than guess, and the caller may name a convention. */
 typedef enum at3r_c2r { AT3R_C2R_MATCH_CUFFT = 0, AT3R_C2R_HERMITIAN = 1, AT3R_C2R_PACKED = 2 } at3r_c2r;
 
 typedef struct at3r_geom {
@@ -76,12 +78,21 @@ typedef struct at3r_geom {
     int c2r;                  /* at3r_c2r (WBP only) */
     int slab_slices;          /* y-slices per device batch; 0 = automatic */
     int compute_rfactor;      /* SART: accumulate per-iteration residual sums */
+    /* SART: seed of the random table of the empty-voxel fill that ends every
+     * reconstruction (CTomoSart::DoIt -> GFillEmpty2D, AreTomo/Recon/
+     * CTomoSart.cpp:88, MaUtil/GFillEmpty2D.cu:7-143): a voxel left at the
+     * -1e30 "empty" value takes the value of the first non-empty voxel along
+     * its chain through the table (entry i drawn from subsequence i of
+     * cuRAND's XORWOW, MaUtil/GGenRandoms.cu:7-49), else the slice mean.  The
+     * reference seeds it with time(0) when it sets up a series;
+     * at3r_geom_init does the same, and a fixed seed makes runs repeatable. */
+    unsigned long long fill_seed;
 } at3r_geom;
 
 typedef struct at3r_plan at3r_plan;
 
 /* Fills g with the reference's defaults for the method (relax = 1/subsets,
- * FP32 storage, cuFFT-matching C2R, automatic slabs). */
+ * FP32 storage, cuFFT-matching C2R, automatic slabs, fill seed = time(0)). */
 void at3r_geom_init(at3r_geom* g, int method);
 
 /* Validates g, uploads the geometry table and allocates the device workspace
@@ -121,6 +132,18 @@ int at3r_plan_kernel_stats(at3r_plan* plan, int kind, const char** name, int64_t
 int64_t at3r_plan_last_launches(const at3r_plan* plan);
 /* Which C2R convention the plan resolved to (AT3R_C2R_HERMITIAN/PACKED). */
 int at3r_plan_c2r(const at3r_plan* plan);
+/* What the last run met, as bits ORed over its slices (waits for the
+ * device): 1 the SART volume held empty (-1e30) voxels, so the forward
+ * projection tested every sample and the fill ran; 2 the staged projections
+ * held values at or below -5e9 (near the -1e10 "missing" test), so the
+ * back-projection tested every sample; 4 the SART residual did; 8 a fill chain
+ * found no non-empty voxel and took the slice mean.  -1 on a CUDA error. */
+int at3r_plan_flags_seen(const at3r_plan* plan);
+/* The SART plan's fill table (see at3r_geom.fill_seed): Nx * Nz entries, entry
+ * i = Z * Nx + X for the voxel at (X, Z) of a slice before the z flip, as
+ * GGenRandoms draws it; n = the capacity in entries.  For checking only: the
+ * reconstruction draws the entries it needs as it goes. */
+at3r_status at3r_plan_fill_table(const at3r_plan* plan, int* table, size_t n);
 
 /* SART of a device-resident series without allocating device memory.  No
  * counterpart in the reference: it is for callers that cannot allocate when
@@ -134,8 +157,11 @@ int at3r_plan_c2r(const at3r_plan* plan);
  * 2 * n_tilts * (nx & ~1) floats for at least one y-slice (and n_tilts <=
  * 4096), otherwise AT3R_ERR_TOO_LARGE.  Calls share that array and it keeps
  * the last call's contents: calls that overlap on the GPU race, so serialise
- * them.  The first call on a device does a one-time set-up (the array's
- * device address, a kernel attribute); make it before any stream capture.
+ * them.  Every call looks up the array's device address on the current
+ * device (cudaGetSymbolAddress); the first call on a device also does a
+ * one-time set-up (a kernel attribute); make that first call before any
+ * stream capture.  The per-tilt table travels to the array in kernel
+ * parameters, so no host buffer has to outlive the call.
  * Enqueues on `stream` and returns without waiting. */
 at3r_status at3r_sart_device_noalloc(const float* proj, int nx, int ny, int n_tilts, const float* tilts_deg,
                                      int vol_z, int start_tilt, int num_tilts, int iterations, int subsets,
@@ -230,7 +256,9 @@ at3r_status at3r_server_create(const at3r_server_opts* opts, at3r_server** out);
 at3r_status at3r_server_submit(at3r_server* server, const at3r_geom* g, const float* const* frames,
                                float* const* vol_frames, int64_t* id);
 /* Blocks until request `id` is done; its status; latency from submission to
- * the volume in host memory, and the part of it spent queued. */
+ * the volume in host memory, and the part of it spent queued.  A request is
+ * waited for once: its id is released on return, and a second concurrent
+ * wait on the same id returns AT3R_ERR_INVALID_ARGUMENT at once. */
 at3r_status at3r_server_wait(at3r_server* server, int64_t id, double* latency_s, double* queued_s);
 /* Device bytes currently admitted (by estimate). */
 size_t at3r_server_in_use_bytes(at3r_server* server);

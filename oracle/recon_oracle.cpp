@@ -21,6 +21,11 @@
 namespace {
 
 int g_c2r_mode = 0;
+// Threads the loops inside one y-slice use.  The *_run entry points spread
+// slices over the threads when there are at least as many slices as threads,
+// and otherwise run the slices one after another with the threads inside each
+// (a 4096-wide SART slice is tens of seconds on one core).
+int g_inner = 1;
 constexpr float kSentinelTest = -1e10f;   // "empty" test used throughout the reference
 constexpr float kSentinelValue = -1e30f;  // value written for an empty result
 
@@ -214,6 +219,7 @@ void bp_wbp_2x(const R* sino, int N, int T, const float* cs, int Nx, int Nz, R* 
     const R cent = (R)(N / 2);
     const float centf = (float)(N / 2);
     const int endX = N - 2;
+#pragma omp parallel for schedule(static) num_threads(g_inner) if (g_inner > 1)
     for (int Z = 0; Z < Z2; Z++) {
         const R fZ = (R)(Z - Nz);
         const float fZf = (float)Z - (float)Z2 / 2.0f;
@@ -228,7 +234,9 @@ void bp_wbp_2x(const R* sino, int N, int T, const float* cs, int Nx, int Nz, R* 
                 if (xf < 0 || xf > endX) continue;
                 const int i = (int)xf;
                 const R xp = (fX * (R)c + fZ * (R)s) / (R)2 + cent + (R)0.5;
-                const R w = xp - i;
+                // where the reference's FP32 fraction is exactly 0 the second
+                // sample has weight 0 (a -1e30 there contributes nothing)
+                const R w = xf == (float)i ? (R)0 : xp - i;
                 const R* p = sino + (size_t)t * N + i;
                 R v = p[0] * (1 - w) + p[1] * w;
                 if (v <= (R)kSentinelTest) continue;
@@ -249,25 +257,34 @@ void fourier_crop(const R* g, int Nx, int Nz, R* f, int mode)
 {
     const int X2 = 2 * Nx, Z2 = 2 * Nz, KX = Nx / 2 + 1;
     std::vector<std::complex<R>> rows((size_t)Z2 * KX);
-    std::vector<std::complex<R>> line(std::max(X2, Z2));
-    for (int Z = 0; Z < Z2; Z++) {
-        for (int X = 0; X < X2; X++) line[X] = std::complex<R>(g[(size_t)Z * X2 + X], 0);
-        fft<R>(line.data(), X2, -1);
-        for (int k = 0; k < KX; k++) rows[(size_t)Z * KX + k] = line[k];
+#pragma omp parallel num_threads(g_inner) if (g_inner > 1)
+    {
+        std::vector<std::complex<R>> line(X2);
+#pragma omp for schedule(static)
+        for (int Z = 0; Z < Z2; Z++) {
+            for (int X = 0; X < X2; X++) line[X] = std::complex<R>(g[(size_t)Z * X2 + X], 0);
+            fft<R>(line.data(), X2, -1);
+            for (int k = 0; k < KX; k++) rows[(size_t)Z * KX + k] = line[k];
+        }
     }
     const R norm = (R)(1.0 / X2 / Z2);
     std::vector<std::complex<R>> crop((size_t)Nz * KX);
-    std::vector<std::complex<R>> col(Z2), col2(Nz);
-    for (int k = 0; k < KX; k++) {
-        for (int Z = 0; Z < Z2; Z++) col[Z] = rows[(size_t)Z * KX + k];
-        fft<R>(col.data(), Z2, -1);
-        for (int kz = 0; kz < Nz; kz++) {
-            int src = kz <= Nz / 2 ? kz : kz + Nz;
-            col2[kz] = col[src] * norm;
+#pragma omp parallel num_threads(g_inner) if (g_inner > 1)
+    {
+        std::vector<std::complex<R>> col(Z2), col2(Nz);
+#pragma omp for schedule(static)
+        for (int k = 0; k < KX; k++) {
+            for (int Z = 0; Z < Z2; Z++) col[Z] = rows[(size_t)Z * KX + k];
+            fft<R>(col.data(), Z2, -1);
+            for (int kz = 0; kz < Nz; kz++) {
+                int src = kz <= Nz / 2 ? kz : kz + Nz;
+                col2[kz] = col[src] * norm;
+            }
+            fft<R>(col2.data(), Nz, +1);
+            for (int z = 0; z < Nz; z++) crop[(size_t)z * KX + k] = col2[z];
         }
-        fft<R>(col2.data(), Nz, +1);
-        for (int z = 0; z < Nz; z++) crop[(size_t)z * KX + k] = col2[z];
     }
+#pragma omp parallel for schedule(static) num_threads(g_inner) if (g_inner > 1)
     for (int z = 0; z < Nz; z++) c2r<R>(&crop[(size_t)z * KX], Nx, f + (size_t)z * Nx, mode);
 }
 
@@ -277,14 +294,18 @@ void wbp_slice(const float* frames, int nx, int ny, int T, const float* cs, int 
 {
     const int N = nx & ~1, Nx = N;
     std::vector<R> sino((size_t)T * N);
-    std::vector<std::complex<R>> work;
-    for (int t = 0; t < T; t++) {
-        const float* src = frames + ((size_t)t * ny + y) * nx;
-        R* row = sino.data() + (size_t)t * N;
-        // AreTomo/Recon/GWeightProjs.cu:18
-        const R wgt = (R)cs[2 * t] / (R)Nz;
-        for (int x = 0; x < N; x++) row[x] = (R)src[x] * wgt;
-        rweight_row<R>(row, N, h, work);
+#pragma omp parallel num_threads(g_inner) if (g_inner > 1)
+    {
+        std::vector<std::complex<R>> work;
+#pragma omp for schedule(static)
+        for (int t = 0; t < T; t++) {
+            const float* src = frames + ((size_t)t * ny + y) * nx;
+            R* row = sino.data() + (size_t)t * N;
+            // AreTomo/Recon/GWeightProjs.cu:18
+            const R wgt = (R)cs[2 * t] / (R)Nz;
+            for (int x = 0; x < N; x++) row[x] = (R)src[x] * wgt;
+            rweight_row<R>(row, N, h, work);
+        }
     }
     std::vector<R> g((size_t)4 * Nx * Nz), f((size_t)Nx * Nz);
     bp_wbp_2x<R>(sino.data(), N, T, cs, Nx, Nz, g.data());
@@ -302,6 +323,7 @@ void bp_sart(const R* sino, int N, const float* cs, int start, int end, R relax,
     const R cent = (R)N / (R)2;
     const float centf = (float)N / 2.0f;
     const int endX = N - 2;
+#pragma omp parallel for schedule(static) num_threads(g_inner) if (g_inner > 1)
     for (int Z = 0; Z < Nz; Z++) {
         const R fZ = (R)Z - (R)Nz * (R)0.5;
         const float fZf = (float)Z - (float)Nz * 0.5f;
@@ -316,7 +338,7 @@ void bp_sart(const R* sino, int N, const float* cs, int start, int end, R relax,
                 if (xf < 0 || xf > endX) continue;
                 const int i = (int)xf;
                 const R xp = fX * (R)c + fZ * (R)s + cent;
-                const R w = xp - i;
+                const R w = xf == (float)i ? (R)0 : xp - i;   // as in bp_wbp_2x
                 const R* p = sino + (size_t)t * N + i;
                 R v = p[0] * (1 - w) + p[1] * w;
                 if (v <= (R)kSentinelTest) continue;
@@ -333,7 +355,8 @@ void bp_sart(const R* sino, int N, const float* cs, int start, int end, R relax,
 
 // Forward projection of tilts [start, end), AreTomo/Recon/GForProj.cu:10-76.
 // The ray length, the in-volume test and the cell index are computed in FP32
-// as the reference does; sample positions' fractions and the sums in R.
+// as the reference does; sample positions' fractions (zero where the FP32
+// fraction is zero) and the sums in R.
 template <class R>
 void forward_project(const R* vol, int Nx, int Nz, int N, const float* cs, int start, int end, R* fp)
 {
@@ -345,6 +368,7 @@ void forward_project(const R* vol, int Nx, int Nz, int N, const float* cs, int s
         const R halfL = (R)L * (R)0.5;
         const float halfLf = (float)L * 0.5f;
         const float tzf = (float)Nz * 0.5f;
+#pragma omp parallel for schedule(static) num_threads(g_inner) if (g_inner > 1)
         for (int u = 0; u < N; u++) {
             const float fXpf = (float)u - 0.5f * (float)N;
             const float txf = fXpf / fc + (float)Nx * 0.5f;
@@ -359,7 +383,10 @@ void forward_project(const R* vol, int Nx, int Nz, int N, const float* cs, int s
                 if (xf < 0 || zf < 0 || xf > endX || zf > endZ) continue;
                 const int ix = (int)xf, iz = (int)zf;
                 const R z0 = (R)i - halfL;
-                const R wx = (tx - z0 * s) - ix, wz = (tz + z0 * c) - iz;
+                // zero where the reference's FP32 fraction is exactly zero, so a
+                // -1e30 voxel of weight 0 adds nothing, as in the reference
+                const R wx = xf == (float)ix ? (R)0 : (tx - z0 * s) - ix;
+                const R wz = zf == (float)iz ? (R)0 : (tz + z0 * c) - iz;
                 const R* v = vol + (size_t)iz * Nx + ix;
                 R val = v[0] * (1 - wx) * (1 - wz) + v[1] * wx * (1 - wz) + v[Nx] * (1 - wx) * wz +
                         v[Nx + 1] * wx * wz;
@@ -370,6 +397,70 @@ void forward_project(const R* vol, int Nx, int Nz, int N, const float* cs, int s
             fp[(size_t)t * N + u] = cnt <= 0 ? (R)kSentinelValue : sum / cnt;
         }
     }
+}
+
+// The fill's random table (MaUtil/GGenRandoms.cu, drawn once per series by
+// CTomoBase::Setup -> GFillEmpty2D::SetSize): entry i = the voxel index the
+// chain of voxel i starts at, for the Nx*Nz voxels of an XZ slice in the
+// reference's order (i = Z*Nx + X, before the z flip).  Set by the caller
+// from the table the device drew (the oracle has no cuRAND); without one,
+// every empty voxel takes the slice mean.
+std::vector<int> g_fill_table;
+
+// MaUtil/GFillEmpty2D.cu:7-143 on one slice vol[Z][X]: voxels below -1e10
+// are empty (mGFindEmpty); the mean of the others is summed in float by one
+// 512-thread block, thread t taking voxels t, t+512, ... in index order, then
+// a tree over the threads (mGCalcMean); an empty voxel follows its chain
+// through the table (at most 100 links) to the first non-empty voxel and
+// takes its value, else the mean (mGFillEmpty2D).  Only empty voxels are
+// written and only non-empty ones read, so the result is order-free.
+template <class R>
+void fill_empty(R* vol, int Nx, int Nz)
+{
+    const int n = Nx * Nz;
+    std::vector<unsigned char> empty(n);
+    bool any = false;
+    for (int i = 0; i < n; i++) {
+        empty[i] = vol[i] < (R)kSentinelTest;
+        any |= empty[i] != 0;
+    }
+    if (!any) return;
+    float s[512], c[512];
+    for (int t = 0; t < 512; t++) {
+        float sum = 0.f, cnt = 0.f;
+        for (int i = t; i < n; i += 512) {
+            if (empty[i]) continue;
+            sum += (float)vol[i];
+            cnt += 1.0f;
+        }
+        s[t] = sum;
+        c[t] = cnt;
+    }
+    for (int off = 256; off > 0; off >>= 1)
+        for (int t = 0; t < off; t++) {
+            s[t] += s[t + off];
+            c[t] += c[t + off];
+        }
+    const R mean = c[0] <= 0.f ? (R)0 : (R)(s[0] / c[0]);
+    const bool chains = (int)g_fill_table.size() == n;
+    std::vector<R> out(vol, vol + n);
+    for (int i = 0; i < n; i++) {
+        if (!empty[i]) continue;
+        R v = mean;
+        if (chains) {
+            int next = g_fill_table[i];
+            for (int j = 0; j < 100; j++) {
+                if (empty[next]) {
+                    next = g_fill_table[next];
+                    continue;
+                }
+                v = vol[next];
+                break;
+            }
+        }
+        out[i] = v;
+    }
+    std::copy(out.begin(), out.end(), vol);
 }
 
 // AreTomo/Util/CSplitItems.cpp:25-48
@@ -416,19 +507,8 @@ void sart_slice(const float* frames, int nx, int ny, int T, const float* cs, int
             bp_sart<R>(fp.data(), N, cs, t0, t1, relax, Nx, Nz, vol.data());
         }
     }
-    // MaUtil/GFillEmpty2D.cu replaces -1e30 voxels with a randomly chosen
-    // valid one; from a zero start no voxel can reach -1e30, so this fill
-    // (deterministic: the mean of valid voxels) is a guard only.
-    double msum = 0;
-    size_t mcnt = 0, empty = 0;
-    for (R v : vol) {
-        if (v < (R)kSentinelTest) empty++;
-        else { msum += v; mcnt++; }
-    }
-    if (empty) {
-        R mean = mcnt ? (R)(msum / mcnt) : (R)0;
-        for (R& v : vol) if (v < (R)kSentinelTest) v = mean;
-    }
+    // CTomoSart.cpp:88: the empty-voxel fill of the slice
+    fill_empty<R>(vol.data(), Nx, Nz);
     for (int z = 0; z < Nz; z++)
         std::memcpy(out + (size_t)(Nz - 1 - z) * Nx, vol.data() + (size_t)z * Nx, sizeof(R) * Nx);
 }
@@ -454,9 +534,12 @@ int wbp_run(const float* frames, int nx, int ny, int T, const float* tilts, int 
     std::vector<R> h;
     rweight_filter<R>(Nx, h);
     get_plan(Nx); get_plan(2 * Nx); get_plan(2 * vol_z); get_plan(vol_z); get_plan(Nx / 2);
-#pragma omp parallel for schedule(dynamic, 1) num_threads(nthreads > 0 ? nthreads : 1)
+    const int nth = nthreads > 0 ? nthreads : 1;
+    g_inner = (y1 - y0) < nth ? nth : 1;
+#pragma omp parallel for schedule(dynamic, 1) num_threads(g_inner > 1 ? 1 : nth)
     for (int y = y0; y < y1; y++)
         wbp_slice<R>(frames, nx, ny, T, cs.data(), vol_z, y, h, out + (size_t)(y - y0) * Nx * vol_z);
+    g_inner = 1;
     return 0;
 }
 
@@ -475,7 +558,8 @@ int sart_run(const float* frames, int nx, int ny, int T, const float* tilts, int
     if (rf) std::memset(rf, 0, sizeof(double) * 2 * iters);
     const int nth = nthreads > 0 ? nthreads : 1;
     std::vector<std::vector<double>> rfs(nth, std::vector<double>(2 * (iters > 0 ? iters : 1), 0.0));
-#pragma omp parallel for schedule(dynamic, 1) num_threads(nth)
+    g_inner = (y1 - y0) < nth ? nth : 1;
+#pragma omp parallel for schedule(dynamic, 1) num_threads(g_inner > 1 ? 1 : nth)
     for (int y = y0; y < y1; y++) {
         int tid = 0;
 #ifdef _OPENMP
@@ -484,6 +568,7 @@ int sart_run(const float* frames, int nx, int ny, int T, const float* tilts, int
         sart_slice<R>(frames, nx, ny, T, cs.data(), vol_z, y, start, num, iters, subsets, rlx,
                       out + (size_t)(y - y0) * Nx * vol_z, rf ? rfs[tid].data() : nullptr);
     }
+    g_inner = 1;
     if (rf)
         for (auto& v : rfs)
             for (int i = 0; i < 2 * iters; i++) rf[i] += v[i];
@@ -768,6 +853,12 @@ float thick_plane_std(const float* vol, int Nx, int Nz, int k, int x0, int tx, i
 }  // namespace
 
 extern "C" {
+
+void oracle_set_fill_table(const int* table, int n)
+{
+    if (table && n > 0) g_fill_table.assign(table, table + n);
+    else g_fill_table.clear();
+}
 
 void oracle_set_c2r_mode(int mode) { g_c2r_mode = mode; }
 int oracle_get_c2r_mode(void) { return g_c2r_mode; }

@@ -51,6 +51,13 @@ int oracle_sart_f32(const float* frames, int nx, int ny, int n_tilts, const floa
                     int vol_z, int start_tilt, int num_tilts, int iters, int subsets, double relax,
                     int y0, int y1, float* out, double* rfactor, int n_threads);
 
+/* The random table of SART's empty-voxel fill (MaUtil/GGenRandoms.cu as
+ * GFillEmpty2D::SetSize draws it: Nx * Nz entries for the XZ slice in the
+ * reference's voxel order, i = Z * Nx + X before the z flip), e.g. the one a
+ * device plan drew; used by oracle_sart_* until replaced.  NULL / n <= 0
+ * clears it: empty voxels then take the slice mean. */
+void oracle_set_fill_table(const int* table, int n);
+
 /* Projection-alignment re-projection of tilt proj_idx
  * (AreTomo/ProjAlign/CCalcReproj.cpp + GReproj.cu): for every row, the tilts
  * of the range CCalcReproj::mFindProjRange picks (skip flags as the caller

@@ -12,6 +12,9 @@
 //          CDoWbpRecon::DoIt / CDoSartRecon::DoIt return them: one XZ slice
 //          per y, z already flipped by the reference)
 // stdout : one JSON line with the wall time of the DoIt call.
+// REF_FILL_SEED (environment, optional): the value time() returns, which
+//          GGenRandoms::DoIt seeds the empty-voxel fill's random table with
+//          (MaUtil/GGenRandoms.cu:42); unset, time() is the clock's.
 #include "AreTomo/Recon/CReconInc.h"
 #include "AreTomo/MrcUtil/CMrcUtilInc.h"
 #include <cuda_runtime.h>
@@ -19,9 +22,25 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <ctime>
 #include <vector>
 
 namespace MAR = McAreTomo::AreTomo::Recon;
+
+static long long g_seed = -1;
+extern "C" time_t time(time_t* t)
+{
+    time_t v;
+    if (g_seed >= 0) {
+        v = (time_t)g_seed;
+    } else {
+        timespec ts{};
+        clock_gettime(CLOCK_REALTIME, &ts);
+        v = ts.tv_sec;
+    }
+    if (t) *t = v;
+    return v;
+}
 
 static bool read_all(FILE* f, void* p, size_t n) { return fread(p, 1, n, f) == n; }
 
@@ -31,6 +50,7 @@ int main(int argc, char** argv)
         fprintf(stderr, "usage: %s wbp|sart in.bin out.bin volZ [start num iters subsets]\n", argv[0]);
         return 2;
     }
+    if (const char* e = getenv("REF_FILL_SEED")) g_seed = atoll(e);
     bool sart = strcmp(argv[1], "sart") == 0;
     if (sart && argc < 9) { fprintf(stderr, "sart needs 8 args\n"); return 2; }
     FILE* fi = fopen(argv[2], "rb");

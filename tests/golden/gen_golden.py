@@ -107,14 +107,24 @@ def read_output(path):
     return vol
 
 
-def run_reference(mode, frames, tilts, vol_z, start=0, ntilts=0, iters=0, subsets=0):
+SHIM_BIN = os.path.join(ROOT, "oracle", "_ref", "shim_recon")
+
+
+def run_reference(mode, frames, tilts, vol_z, start=0, ntilts=0, iters=0, subsets=0, fill_seed=None, binary=None):
+    """fill_seed: the seed the reference's empty-voxel fill table is drawn
+    with (the driver's time()); None: the clock, as in the reference.
+    binary: another build of the same driver (SHIM_BIN: the drop-in shim's
+    CDoWbpRecon / CDoSartRecon over libat3r); default the reference's."""
     with tempfile.TemporaryDirectory() as td:
         fin, fout = os.path.join(td, "in.bin"), os.path.join(td, "out.bin")
         write_input(fin, frames, tilts)
-        args = [REF_BIN, mode, fin, fout, str(vol_z)]
+        args = [binary or REF_BIN, mode, fin, fout, str(vol_z)]
         if mode == "sart":
             args += [str(start), str(ntilts), str(iters), str(subsets)]
-        r = subprocess.run(args, capture_output=True, text=True, check=True)
+        env = dict(os.environ)
+        if fill_seed is not None:
+            env["REF_FILL_SEED"] = str(int(fill_seed))
+        r = subprocess.run(args, capture_output=True, text=True, check=True, env=env)
         line = [ln for ln in r.stdout.splitlines() if ln.startswith("{")][-1]
         return read_output(fout), json.loads(line)
 

@@ -24,6 +24,7 @@ def lib():
                                          ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double,
                                          ctypes.c_int, ctypes.c_int, P, P, ctypes.c_int]
         _lib.oracle_sart_f32.argtypes = _lib.oracle_sart_f64.argtypes
+        _lib.oracle_set_fill_table.argtypes = [P, ctypes.c_int]
     return _lib
 
 
@@ -47,7 +48,9 @@ def wbp(frames, tilts, vol_z, y0=0, y1=None, c2r_mode=0, f32=False, threads=os.c
 
 
 def sart(frames, tilts, vol_z, start, ntilts, iters, subsets, relax=0.0, y0=0, y1=None, f32=False,
-         threads=os.cpu_count(), rfactor=False):
+         threads=os.cpu_count(), rfactor=False, fill_table=None):
+    """fill_table: the random table of the empty-voxel fill (Nx * vol_z
+    entries, as a device plan drew it); None: empty voxels take the mean."""
     frames = np.ascontiguousarray(frames, np.float32)
     tilts = np.ascontiguousarray(tilts, np.float32)
     t, ny, nx = frames.shape
@@ -55,9 +58,15 @@ def sart(frames, tilts, vol_z, start, ntilts, iters, subsets, relax=0.0, y0=0, y
     out = np.zeros((y1 - y0, vol_z, nx & ~1), np.float32 if f32 else np.float64)
     rf = np.zeros(2 * max(iters, 1), np.float64)
     L = lib()
+    if fill_table is None:
+        L.oracle_set_fill_table(None, 0)
+    else:
+        tab = np.ascontiguousarray(fill_table, np.int32)
+        L.oracle_set_fill_table(_p(tab), int(tab.size))
     fn = L.oracle_sart_f32 if f32 else L.oracle_sart_f64
     rc = fn(_p(frames), nx, ny, t, _p(tilts), vol_z, start, ntilts, iters, subsets, relax, y0, y1, _p(out),
             _p(rf), threads)
+    L.oracle_set_fill_table(None, 0)
     if rc != 0:
         raise ValueError(f"oracle sart rc={rc}")
     return (out, rf[: 2 * iters].reshape(iters, 2)) if rfactor else out
