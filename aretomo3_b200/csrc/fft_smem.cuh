@@ -20,21 +20,12 @@ namespace at3r {
 
 constexpr int kMaxFftStages = 32;
 
-// Element i of a sequence in shared memory sits at fft_pad(i): within each
-// block of 16 elements (128 bytes, every bank once for 8-byte elements) the
-// index is XORed with a pattern taken from the block number b = i / 16 —
-// bits 0-2 of b in bits 0-2, bit 2 of b in bit 3.  A run of 16 consecutive
-// elements in one block still meets every bank once (the butterflies' reads
-// and the wide stages' writes), while the strided writes of the early
-// Stockham stages — groups of Ns < 16 consecutive elements spaced Ns * R
-// apart — land in different banks: for Ns = 1 the eight blocks a half-warp
-// touches differ in bits 0-2, for Ns = 8 the two groups differ in bit 3.
-// Shared-memory replay of every stage of the row and column lengths of the
-// reconstruction (8192, 4096, 2400, 1200, ...) gives 1.0-1.1 wavefronts per
-// ideal wavefront, against 1.1-1.6 for one spare element per 16.
-__host__ __device__ constexpr int fft_pad(int i) { return i ^ (((i >> 4) & 7) | ((i >> 3) & 8)); }
-// Elements one sequence of length n occupies (whole blocks of 16).
-__host__ __device__ constexpr int fft_pitch(int n) { return (n + 15) & ~15; }
+// Sequences sit in shared memory with one spare element after every 16, so
+// that the stride-R writes of the early Stockham stages (and other strided
+// patterns) spread over the banks: element i of a sequence is at fft_pad(i).
+__host__ __device__ constexpr int fft_pad(int i) { return i + (i >> 4); }
+// Elements one padded sequence of length n occupies.
+__host__ __device__ constexpr int fft_pitch(int n) { return n + ((n - 1) >> 4) + 1; }
 
 struct FftDirect {
     int n;                       // length
