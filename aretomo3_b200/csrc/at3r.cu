@@ -13,6 +13,7 @@
 #include <ctime>
 #include <complex>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <mutex>
@@ -113,6 +114,7 @@ struct at3r_plan {
     int rs_zcrop = 0;                           // radix set of the z-crop kernel (both its lengths)
     size_t smem_rweight = 0, smem_row = 0, smem_zcrop = 0, smem_xc2r = 0;
     int bp_ww_sart = 0, bp_ww_wbp = 0;
+    int bp_bulk = 0;   // FP32 back-projection staging by bulk asynchronous copies (AT3R_BP_BULK_STAGING)
     // host path
     float* d_proj_slab[2] = {nullptr, nullptr};
     float* d_vol_slab[2] = {nullptr, nullptr};
@@ -221,7 +223,18 @@ int bp_window(int tx, int tz, double scale, const std::vector<float>& cs, int T)
 }
 
 // tilts are staged in chunks, so the window buffer does not grow with the tilt count
-size_t bp_smem(int, int ww) { return bp_smem_bytes(ww); }
+// dynamic shared memory of a back-projection launch (bulk: the bulk-copy
+// staging's raw rows and mbarrier on top)
+size_t bp_smem(int bulk) { return bp_smem_bytes(bulk); }
+
+// Back-projection window staging by bulk asynchronous copies (FP32 storage,
+// N a multiple of 4): off unless AT3R_BP_BULK_STAGING=1 at plan creation; an
+// alternative to the load path, kept for comparison.
+bool bp_bulk_from_env()
+{
+    const char* e = std::getenv("AT3R_BP_BULK_STAGING");
+    return e && e[0] == '1';
+}
 
 // Every plan raises a kernel's dynamic shared-memory limit to the device
 // maximum (once per kernel and device), so plans of different sizes can
@@ -328,13 +341,16 @@ at3r_status run_slab_t(at3r_plan* p, const float* proj, size_t tilt_stride, int 
         BpArgs a{};
         a.T = T; a.N = N; a.cs = p->d_cs; a.GX = Nx; a.GZ = Nz; a.S = S;
         a.out = reinterpret_cast<float*>(p->d_w); a.out_slice = (size_t)Nx * Nz; a.ww = p->bp_ww_sart;
-        a.flags = p->d_flags; a.seen = p->d_seen;
+        a.flags = p->d_flags; a.seen = p->d_seen; a.bulk = p->bp_bulk;
         a.scale = p->d_scale; a.shadow = p->d_shadow;
         const dim3 bgrid((Nx + BP_TX - 1) / BP_TX, (Nz + BP_TZ - 1) / BP_TZ, SG);
+        auto bp_launch = [&](int nt_) {
+            k_bp<0, ST, VT, true><<<bgrid, BP_THREADS, bp_smem(a.bulk), st>>>(a);
+        };
         // first back-projection: all tilts, relax 1 (CTomoSart.cpp:68-69)
         a.sino = raw; a.t0 = 0; a.t1 = T; a.relax = 1.f; a.low_bit = kFlagRawLow;
         TB(p, st);
-        k_bp<0, ST, VT, true><<<bgrid, BP_THREADS, bp_smem(T, a.ww), st>>>(a);
+        bp_launch(T);
         TE(p, st, KK_BP_SART, es * S * (double)T * N + (2 * f4 + (vs < 4 ? vs : 0)) * vox, vox * T);
         a.sino = dif; a.relax = p->relax; a.low_bit = kFlagDiffLow;
         for (int it = 0; it < p->g.iterations; it++) {
@@ -352,7 +368,7 @@ at3r_status run_slab_t(at3r_plan* p, const float* proj, size_t tilt_stride, int 
                 TE(p, st, KK_FP_DIFF, vs * vox + 2.0 * es * S * nt * N, samples * N * S);
                 a.t0 = t0; a.t1 = t0 + nt;
                 TB(p, st);
-                k_bp<0, ST, VT, true><<<bgrid, BP_THREADS, bp_smem(nt, a.ww), st>>>(a);
+                bp_launch(nt);
                 TE(p, st, KK_BP_SART, es * S * (double)nt * N + (2 * f4 + (vs < 4 ? vs : 0)) * vox, vox * nt);
             }
         }
@@ -382,10 +398,10 @@ at3r_status run_slab_t(at3r_plan* p, const float* proj, size_t tilt_stride, int 
     BpArgs a{};
     a.sino = filt; a.scale = scale; a.shadow = nullptr; a.T = T; a.N = N; a.t0 = 0; a.t1 = T; a.cs = p->d_cs;
     a.GX = 2 * Nx; a.GZ = 2 * Nz; a.S = S; a.relax = 1.f; a.out = g2; a.out_slice = (size_t)4 * Nx * Nz;
-    a.ww = p->bp_ww_wbp; a.flags = flags; a.seen = p->d_seen; a.low_bit = kFlagRawLow;
-    const dim3 bgrid((2 * Nx + BP_TX - 1) / BP_TX, (2 * Nz + BP_TZ - 1) / BP_TZ, SG);
+    a.ww = p->bp_ww_wbp; a.flags = flags; a.seen = p->d_seen; a.low_bit = kFlagRawLow; a.bulk = p->bp_bulk;
     TB(p, st);
-    k_bp<1, ST, float, false><<<bgrid, BP_THREADS, bp_smem(T, a.ww), st>>>(a);
+    k_bp<1, ST, float, false><<<dim3((2 * Nx + BP_TX - 1) / BP_TX, (2 * Nz + BP_TZ - 1) / BP_TZ, SG), BP_THREADS,
+                                bp_smem(a.bulk), st>>>(a);
     TE(p, st, KK_BP_WBP, es * S * (double)T * N + f4 * 4 * vox, 4 * vox * T);
     TB(p, st);
     dispatch_rs(p->f2x.rs, [&](auto R) {
@@ -425,7 +441,7 @@ at3r_status run_slab(at3r_plan* p, const float* proj, size_t tilt_stride, int pr
 at3r_status ensure_lane2(at3r_plan* p)
 {
     if (p->s_lane2) return AT3R_OK;
-    const size_t S = p->slab, T = p->T, N = p->N, Nx = p->Nx, Nz = p->Nz, KX = p->KX;
+    const size_t S = p->slab_cap, T = p->T, N = p->N, Nx = p->Nx, Nz = p->Nz, KX = p->KX;
     at3r_status rc;
     if ((rc = dalloc_bytes(p, &p->lane2.filt, S * T * N * p->esz))) return rc;
     if (p->g.storage != AT3R_STORE_F32 && (rc = dalloc(p, &p->lane2.scale, S * T))) return rc;
@@ -538,6 +554,45 @@ size_t at3r_plan_estimate_bytes(const at3r_geom* g)
     return work + host_path + tables + T * 8 + (1 << 20);
 }
 
+}  // extern "C"
+
+// The serving loop's view of a request (csrc/at3r_server.cpp): its device
+// bytes — the plan's workspace on one lane, FFT tables, the projections held
+// on the device for the whole request, two volume slabs — and its slab.
+size_t at3r_estimate_resident_bytes(const at3r_geom* g, int* slab_out)
+{
+    if (!g || g->nx < 1 || g->ny < 1 || g->n_tilts < 1 || g->vol_z < 1) return 0;
+    const size_t T = g->n_tilts, N = g->nx & ~1, Nx = N, Nz = g->vol_z, KX = Nx / 2 + 1, nx = g->nx, ny = g->ny;
+    const size_t esz = g->storage == AT3R_STORE_F32 ? 4 : 2;
+    size_t per_slice, tables = 0, work;
+    if (g->method == AT3R_SART) {
+        per_slice = 2 * T * N * esz + 4 * Nx * Nz + (esz < 4 ? 2 * Nx * Nz + 4 * T : 0);
+    } else {
+        per_slice = T * N * sizeof(float) + 16 * Nx * Nz + 2 * Nz * KX * sizeof(float2);
+        tables = 4 * sizeof(float2) * 4 * (N + 2 * Nx + 3 * Nz + Nx);
+    }
+    size_t slab = g->slab_slices > 0 ? (size_t)g->slab_slices : (size_t)default_slab(g, per_slice, 148);
+    slab = std::min<size_t>(slab, ny);
+    if (g->method == AT3R_SART)
+        work = (slab + 7) * (2 * T * N * esz + 4 * Nx * Nz + (esz < 4 ? 2 * Nx * Nz + T * 4 : 0)) + slab * 8;
+    else
+        work = slab * (T * N * esz + 16 * Nx * Nz + 2 * Nz * KX * sizeof(float2) + (esz < 4 ? T * 4 : 0) + 4);
+    if (slab_out) *slab_out = (int)slab;
+    return work + tables + T * ny * nx * sizeof(float) + 2 * slab * Nx * Nz * sizeof(float) + T * 8 + (1 << 20);
+}
+
+// Rows [y0, y0 + n) of a series held on the device, proj[T][ny][nx], into
+// vol_rows[n][Nz][Nx] on `st`: one slab of the plan's y loop, with none of a
+// run's bookkeeping (timing, R-factor, the run summary).  n <= the plan's slab.
+at3r_status at3r_plan_run_slab(at3r_plan* p, const float* proj, int y0, int n, float* vol_rows, cudaStream_t st)
+{
+    if (!p || !proj || !vol_rows || y0 < 0 || n < 1 || y0 + n > p->ny || n > p->slab_cap)
+        return set_err(AT3R_ERR_INVALID_ARGUMENT, "slab outside the series or the plan's workspace");
+    return run_slab(p, proj, (size_t)p->ny * p->nx, y0, n, vol_rows, st);
+}
+
+extern "C" {
+
 at3r_status plan_create_impl(const at3r_geom* g, cudaStream_t alloc_stream, at3r_plan** out)
 {
     if (!g || !out) return set_err(AT3R_ERR_INVALID_ARGUMENT, "null argument");
@@ -570,6 +625,7 @@ at3r_status plan_create_impl(const at3r_geom* g, cudaStream_t alloc_stream, at3r
     p->g.tilts_deg = p->tilts.data();
     p->nx = g->nx; p->ny = g->ny; p->T = g->n_tilts;
     p->fill_seed = g->fill_seed;
+    p->bp_bulk = g->storage == AT3R_STORE_F32 && bp_bulk_from_env() ? 1 : 0;
     p->N = g->nx & ~1; p->Nx = p->N; p->Nz = g->vol_z; p->KX = p->Nx / 2 + 1;
     cudaGetDevice(&p->device);
 
@@ -607,7 +663,7 @@ at3r_status plan_create_impl(const at3r_geom* g, cudaStream_t alloc_stream, at3r
         if (p->bp_ww_sart > BP_WW) return fail(set_err(AT3R_ERR_TOO_LARGE, "back-projection window exceeds its stride"));
         for (const void* fn : {(const void*)k_bp<0, float, float, true>, (const void*)k_bp<0, __half, __half, true>,
                                (const void*)k_bp<0, __nv_bfloat16, __nv_bfloat16, true>})
-            if ((rc = set_smem(fn, bp_smem(p->T, p->bp_ww_sart)))) return fail(rc);
+            if ((rc = set_smem(fn, bp_smem(p->bp_bulk)))) return fail(rc);
         per_slice = 2 * T * N * p->esz + 4 * Nx * Nz + (p->esz < 4 ? 2 * Nx * Nz + 4 * T : 0);
     } else {
         if (g->c2r == AT3R_C2R_MATCH_CUFFT) {
@@ -661,7 +717,7 @@ at3r_status plan_create_impl(const at3r_geom* g, cudaStream_t alloc_stream, at3r
             if ((rc = set_smem(f.first, f.second))) return fail(rc);
         for (const void* fn : {(const void*)k_bp<1, float, float, false>, (const void*)k_bp<1, __half, float, false>,
                                (const void*)k_bp<1, __nv_bfloat16, float, false>})
-            if ((rc = set_smem(fn, bp_smem(p->T, p->bp_ww_wbp)))) return fail(rc);
+            if ((rc = set_smem(fn, bp_smem(p->bp_bulk)))) return fail(rc);
         // R-weight transfer function (GRWeight.cu:15-20), 1/N folded in
         std::vector<float> h(N / 2 + 1);
         const double twopi = (double)6.2831852f;
@@ -1360,7 +1416,7 @@ extern "C" at3r_status at3r_sart_device_noalloc(const float* proj, int nx, int n
     }
     const int ww = bp_window(BP_TX, BP_TZ, 1.0, cs, T);
     if (ww > BP_WW) return set_err(AT3R_ERR_TOO_LARGE, "back-projection window exceeds its stride");
-    if (bp_smem(T, ww) > 227 * 1024) return set_err(AT3R_ERR_TOO_LARGE, "back-projection window exceeds 227 KB");
+    if (bp_smem(0) > 227 * 1024) return set_err(AT3R_ERR_TOO_LARGE, "back-projection window exceeds 227 KB");
     unsigned char* base = nullptr;
     at3r_status rc = noalloc_scratch_address(&base);
     if (rc != AT3R_OK) return rc;
@@ -1401,7 +1457,7 @@ extern "C" at3r_status at3r_sart_device_noalloc(const float* proj, int nx, int n
         a.out = v; a.out_slice = (size_t)Nx * Nz; a.ww = ww; a.flags = d_flags;
         const dim3 bgrid((Nx + BP_TX - 1) / BP_TX, (Nz + BP_TZ - 1) / BP_TZ, SG);
         a.sino = d_raw; a.t0 = 0; a.t1 = T; a.relax = 1.f; a.low_bit = kFlagRawLow;
-        k_bp<0, float, float, false><<<bgrid, BP_THREADS, bp_smem(T, ww), st>>>(a);
+        k_bp<0, float, float, false><<<bgrid, BP_THREADS, bp_smem(0), st>>>(a);
         AT3R_CUDA(cudaGetLastError());
         a.sino = d_diff; a.relax = rlx; a.low_bit = kFlagDiffLow;
         for (int it = 0; it < iterations; it++) {
@@ -1413,7 +1469,7 @@ extern "C" at3r_status at3r_sart_device_noalloc(const float* proj, int nx, int n
                                                                                        d_flags);
                 AT3R_CUDA(cudaGetLastError());
                 a.t0 = t0; a.t1 = t0 + nt;
-                k_bp<0, float, float, false><<<bgrid, BP_THREADS, bp_smem(nt, ww), st>>>(a);
+                k_bp<0, float, float, false><<<bgrid, BP_THREADS, bp_smem(0), st>>>(a);
                 AT3R_CUDA(cudaGetLastError());
             }
         }
@@ -1438,6 +1494,19 @@ struct at3r_batch {
     cudaGraphExec_t exec = nullptr;
     std::vector<cudaStream_t> streams;
     std::vector<cudaEvent_t> events;
+    int mode_req = AT3R_BATCH_AUTO, mode = 0;   // requested and chosen form
+    float ms_waves = 0.f, ms_branches = 0.f;    // the autotuner's timings (both forms possible)
+    // WBP batches of one storage type: persistent stage kernels over waves
+    bool waves = false;
+    int storage = 0;
+    int rs[kWbpStages] = {};            // radix set of each FFT stage over the batch
+    size_t smem[kWbpStages] = {};       // dynamic shared memory of each stage
+    int grid[kWbpStages] = {};          // persistent CTAs of each stage
+    std::vector<int> wave_off, wave_n;  // per wave: first descriptor, descriptors
+    std::vector<int> wave_start;        // per (wave, stage): offset of its block-start array
+    WbpSlab* d_slabs = nullptr;
+    int* d_start = nullptr;
+    int* d_counters = nullptr;          // one per (wave, stage)
 };
 
 namespace {
@@ -1450,6 +1519,171 @@ std::map<std::vector<int>, int> g_tune_cache;
 std::vector<int> tune_key(const at3r_plan* p)
 {
     return {p->g.method, p->nx, p->Nz, p->T, p->g.storage, p->g.iterations, (int)p->sub_size.size(), p->slab_cap};
+}
+
+// The five stage kernels of a wave for storage ST, each with the radix set the
+// batch needs; fn[k] for stage k (0 rweight, 1 bp, 2 row_r2c, 3 zcrop, 4 x_c2r).
+template <typename ST>
+void wave_kernels(const int* rs, const void** fn)
+{
+    dispatch_rs(rs[0], [&](auto R) { fn[0] = (const void*)k_wbp_wave<0, ST, decltype(R)::value>; });
+    fn[1] = (const void*)k_wbp_wave<1, ST, 0>;
+    dispatch_rs(rs[2], [&](auto R) { fn[2] = (const void*)k_wbp_wave<2, float, decltype(R)::value>; });
+    dispatch_rs(rs[3], [&](auto R) { fn[3] = (const void*)k_wbp_wave<3, float, decltype(R)::value>; });
+    dispatch_rs(rs[4], [&](auto R) { fn[4] = (const void*)k_wbp_wave<4, float, decltype(R)::value>; });
+}
+
+void wave_kernels_of(int storage, const int* rs, const void** fn)
+{
+    if (storage == AT3R_STORE_F16) wave_kernels<__half>(rs, fn);
+    else if (storage == AT3R_STORE_BF16) wave_kernels<__nv_bfloat16>(rs, fn);
+    else wave_kernels<float>(rs, fn);
+}
+
+// Descriptors of every wave of a WBP batch: wave w holds slab w of every
+// series that has one.  Uploads them with the block-start arrays.
+at3r_status build_waves(at3r_batch* b)
+{
+    const int n = (int)b->plans.size();
+    for (at3r_plan* p : b->plans)
+        if (p->ny > p->slab) {
+            at3r_status rc = ensure_lane2(p);
+            if (rc) return rc;
+        }
+    // as many waves as the series with the most slabs has slabs; every other
+    // series spreads its slabs evenly over them (slab j of n in wave
+    // floor(j * waves / n)), so the waves carry similar work
+    int nw = 0;
+    for (at3r_plan* p : b->plans) nw = std::max(nw, (p->ny + p->slab - 1) / p->slab);
+    std::vector<WbpSlab> slabs;
+    std::vector<int> starts;
+    for (int w = 0; w < nw; w++) {
+        b->wave_off.push_back((int)slabs.size());
+        int cnt = 0;
+        for (int i = 0; i < n; i++) {
+            at3r_plan* p = b->plans[i];
+            const int ns = (p->ny + p->slab - 1) / p->slab;
+            // the slab of series i in wave w, if any: the j with floor(j * nw / ns) == w
+            const int j = (int)(((long long)w * ns + nw - 1) / nw);
+            if (j >= ns || (long long)j * nw / ns != w) continue;
+            const int y0 = j * p->slab;
+            const int S = std::min(p->slab, p->ny - y0);
+            const int Nx = p->Nx, Nz = p->Nz, T = p->T, N = p->N, KX = p->KX;
+            // alternate waves use the plan's two workspaces, so two waves overlap
+            const bool l2 = (w & 1) && p->s_lane2;
+            void* const filt = l2 ? p->lane2.filt : p->d_filt;
+            float* const scale = l2 ? p->lane2.scale : p->d_scale;
+            int* const flags = l2 ? p->lane2.flags : p->d_flags;
+            float* const g2 = l2 ? p->lane2.g2 : p->d_g2;
+            float2* const yw = l2 ? p->lane2.y : p->d_y;
+            WbpSlab d{};
+            d.proj = b->proj[i];
+            d.tilt_stride = (size_t)p->ny * p->nx;
+            d.row_pitch = p->nx;
+            d.y0 = y0;
+            d.cs = p->d_cs;
+            d.T = T; d.N = N; d.Nx = Nx; d.Nz = Nz; d.S = S;
+            d.h = p->d_h;
+            d.filt = filt;
+            d.scale = scale;
+            d.flags = flags;
+            d.g2 = g2;
+            d.y = yw;
+            d.vol = b->vol[i] + (size_t)y0 * Nx * Nz;
+            d.vol_slice = (size_t)Nx * Nz;
+            d.b_rweight = p->b_rweight; d.b_row = p->b_row; d.b_xc2r = p->b_xc2r;
+            d.zcrop_cb = p->zcrop_cb; d.zcrop_pitch = p->zcrop_pitch;
+            d.packed = p->c2r == AT3R_C2R_PACKED;
+            d.norm = (float)(1.0 / (2.0 * Nx) / (2.0 * Nz));
+            BpArgs& a = d.bp;
+            a.sino = filt; a.scale = scale; a.shadow = nullptr; a.T = T; a.N = N; a.t0 = 0; a.t1 = T;
+            a.cs = p->d_cs; a.GX = 2 * Nx; a.GZ = 2 * Nz; a.S = S; a.relax = 1.f; a.out = g2;
+            a.out_slice = (size_t)4 * Nx * Nz; a.ww = p->bp_ww_wbp; a.flags = flags; a.seen = p->d_seen;
+            a.low_bit = kFlagRawLow; a.bulk = 0;
+            d.fN = p->fN.plan; d.f2x = p->f2x.plan; d.f2z = p->f2z.plan; d.fz = p->fz.plan; d.fx = p->fx.plan;
+            d.gx[0] = ((T + 1) / 2 + p->b_rweight - 1) / p->b_rweight;
+            d.gx[1] = (2 * Nx + BP_TX - 1) / BP_TX;
+            d.bp_gy = (2 * Nz + BP_TZ - 1) / BP_TZ;
+            d.bp_gz = (S + SB - 1) / SB;
+            d.gx[2] = (Nz + p->b_row - 1) / p->b_row;
+            d.gx[3] = (KX + p->zcrop_cb - 1) / p->zcrop_cb;
+            d.gx[4] = ((Nz + 1) / 2 + p->b_xc2r - 1) / p->b_xc2r;
+            slabs.push_back(d);
+            cnt++;
+        }
+        b->wave_n.push_back(cnt);
+        // block starts of each stage over this wave's descriptors
+        for (int k = 0; k < kWbpStages; k++) {
+            b->wave_start.push_back((int)starts.size());
+            int acc = 0;
+            for (int j = 0; j < cnt; j++) {
+                const WbpSlab& d = slabs[b->wave_off[w] + j];
+                starts.push_back(acc);
+                acc += k == 1 ? d.gx[1] * d.bp_gy * d.bp_gz : d.gx[k] * d.S;
+            }
+            starts.push_back(acc);
+        }
+    }
+    AT3R_CUDA(cudaMalloc(&b->d_slabs, sizeof(WbpSlab) * slabs.size()));
+    AT3R_CUDA(cudaMalloc(&b->d_start, sizeof(int) * starts.size()));
+    AT3R_CUDA(cudaMalloc(&b->d_counters, sizeof(int) * (size_t)nw * kWbpStages));
+    AT3R_CUDA(cudaMemcpy(b->d_slabs, slabs.data(), sizeof(WbpSlab) * slabs.size(), cudaMemcpyHostToDevice));
+    AT3R_CUDA(cudaMemcpy(b->d_start, starts.data(), sizeof(int) * starts.size(), cudaMemcpyHostToDevice));
+    // radix sets, shared memory and persistent grids of the stage kernels
+    for (at3r_plan* p : b->plans) {
+        b->rs[0] = std::max(b->rs[0], p->fN.rs);
+        b->rs[2] = std::max(b->rs[2], p->f2x.rs);
+        b->rs[3] = std::max(b->rs[3], p->rs_zcrop);
+        b->rs[4] = std::max(b->rs[4], p->fx.rs);
+        b->smem[0] = std::max(b->smem[0], p->smem_rweight);
+        b->smem[2] = std::max(b->smem[2], p->smem_row);
+        b->smem[3] = std::max(b->smem[3], p->smem_zcrop);
+        b->smem[4] = std::max(b->smem[4], p->smem_xc2r);
+    }
+    b->smem[1] = bp_smem(0);
+    const void* fn[kWbpStages];
+    wave_kernels_of(b->storage, b->rs, fn);
+    int dev = 0, sms = 148;
+    AT3R_CUDA(cudaGetDevice(&dev));
+    AT3R_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    for (int k = 0; k < kWbpStages; k++) {
+        at3r_status rc = set_smem(fn[k], b->smem[k]);
+        if (rc) return rc;
+        int per_sm = 0;
+        AT3R_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn[k], k == 1 ? BP_THREADS : 512, b->smem[k]));
+        b->grid[k] = std::max(1, per_sm) * sms;
+    }
+    b->waves = true;
+    return AT3R_OK;
+}
+
+// One run of a wave batch: per wave the flags, then the five stages; even
+// waves on st0, odd ones on st1 (their own workspaces), which both start
+// after the counters are cleared on st0.
+at3r_status run_waves(at3r_batch* b, cudaStream_t st0, cudaStream_t st1, cudaEvent_t ev)
+{
+    const void* fn[kWbpStages];
+    wave_kernels_of(b->storage, b->rs, fn);
+    AT3R_CUDA(cudaMemsetAsync(b->d_counters, 0, sizeof(int) * b->wave_n.size() * kWbpStages, st0));
+    if (st1 != st0) {
+        AT3R_CUDA(cudaEventRecord(ev, st0));
+        AT3R_CUDA(cudaStreamWaitEvent(st1, ev, 0));
+    }
+    for (size_t w = 0; w < b->wave_n.size(); w++) {
+        const cudaStream_t st = (w & 1) ? st1 : st0;
+        const int nw = b->wave_n[w];
+        WbpSlab* ds = b->d_slabs + b->wave_off[w];
+        k_wave_flags<<<nw, 128, 0, st>>>(ds);
+        AT3R_CUDA(cudaGetLastError());
+        for (int k = 0; k < kWbpStages; k++) {
+            const int* start = b->d_start + b->wave_start[w * kWbpStages + k];
+            int* counter = b->d_counters + w * kWbpStages + k;
+            int nslabs = nw;
+            void* args[] = {(void*)&ds, (void*)&start, (void*)&nslabs, (void*)&counter};
+            AT3R_CUDA(cudaLaunchKernel(fn[k], dim3(b->grid[k]), dim3(k == 1 ? BP_THREADS : 512), args, b->smem[k], st));
+        }
+    }
+    return AT3R_OK;
 }
 
 }  // namespace
@@ -1531,6 +1765,18 @@ at3r_status at3r_batch_create(at3r_plan* const* plans, const float* const* proj,
     b->proj.assign(proj, proj + n);
     b->vol.assign(vol, vol + n);
     b->branches = std::max(1, std::min(branches, n));
+    // WBP series of one storage type run as waves of persistent stage kernels
+    bool waves = true;
+    for (int i = 0; i < n; i++)
+        waves = waves && plans[i]->g.method == AT3R_WBP && plans[i]->g.storage == plans[0]->g.storage;
+    if (waves) {
+        b->storage = plans[0]->g.storage;
+        const at3r_status rc = build_waves(b);
+        if (rc) {
+            at3r_batch_destroy(b);
+            return rc;
+        }
+    }
     *out = b;
     return AT3R_OK;
 }
@@ -1538,43 +1784,122 @@ at3r_status at3r_batch_create(at3r_plan* const* plans, const float* const* proj,
 // Captures (on first use) every plan's launches into one graph — plan i on
 // branch i % branches, forked from and joined back to `stream` — and then
 // replays the whole batch as one graph launch.
+// Captures the batch's work into one graph: the wave form (persistent stage
+// kernels over all series) or the branch form (every plan's own launches,
+// plan i on branch i % branches).
+static at3r_status capture_batch(at3r_batch* b, bool waves, cudaGraph_t* graph, cudaGraphExec_t* exec)
+{
+    cudaStream_t cap = nullptr;
+    AT3R_CUDA(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
+    if (b->streams.empty()) {
+        b->streams.assign(b->branches, nullptr);
+        b->events.assign(b->branches + 2, nullptr);
+        for (auto& s2 : b->streams) AT3R_CUDA(cudaStreamCreateWithFlags(&s2, cudaStreamNonBlocking));
+        for (auto& e : b->events) AT3R_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    }
+    AT3R_CUDA(cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal));
+    at3r_status rc = AT3R_OK;
+    if (cudaEventRecord(b->events[0], cap) != cudaSuccess) rc = AT3R_ERR_CUDA;
+    for (int k = 0; k < b->branches && !rc; k++)
+        if (cudaStreamWaitEvent(b->streams[k], b->events[0], 0) != cudaSuccess) rc = AT3R_ERR_CUDA;
+    if (!rc && waves) {
+        // alternate waves on two branches (the plans' two workspaces)
+        rc = run_waves(b, b->streams[0], b->streams[std::min(1, b->branches - 1)], b->events[b->branches + 1]);
+    } else {
+        for (size_t i = 0; i < b->plans.size() && !rc; i++)
+            rc = at3r_run_device(b->plans[i], b->proj[i], b->vol[i], b->streams[i % b->branches]);
+    }
+    for (int k = 0; k < b->branches && !rc; k++) {
+        if (cudaEventRecord(b->events[k + 1], b->streams[k]) != cudaSuccess ||
+            cudaStreamWaitEvent(cap, b->events[k + 1], 0) != cudaSuccess)
+            rc = AT3R_ERR_CUDA;
+    }
+    cudaGraph_t g = nullptr;
+    const cudaError_t ce = cudaStreamEndCapture(cap, &g);
+    cudaStreamDestroy(cap);
+    if (rc || ce != cudaSuccess) {
+        if (g) cudaGraphDestroy(g);
+        cudaGetLastError();
+        return set_err(AT3R_ERR_CUDA, std::string("batch capture failed: ") +
+                                          (rc ? at3r_last_error() : cudaGetErrorString(ce)));
+    }
+    *graph = g;
+    AT3R_CUDA(cudaGraphInstantiate(exec, g, 0));
+    return AT3R_OK;
+}
+
+// Device milliseconds of one launch of a captured batch (after one untimed launch).
+static at3r_status time_graph(cudaGraphExec_t exec, cudaStream_t st, float* ms)
+{
+    cudaEvent_t e0, e1;
+    AT3R_CUDA(cudaEventCreate(&e0));
+    AT3R_CUDA(cudaEventCreate(&e1));
+    cudaGraphLaunch(exec, st);
+    cudaEventRecord(e0, st);
+    cudaGraphLaunch(exec, st);
+    cudaEventRecord(e1, st);
+    const cudaError_t e = cudaEventSynchronize(e1);
+    cudaEventElapsedTime(ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    AT3R_CUDA(e);
+    return AT3R_OK;
+}
+
 at3r_status at3r_batch_run(at3r_batch* b, void* stream)
 {
     if (!b) return set_err(AT3R_ERR_INVALID_ARGUMENT, "null batch");
     cudaStream_t st = (cudaStream_t)stream;
     if (!b->exec) {
-        cudaStream_t cap = nullptr;
-        AT3R_CUDA(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
-        b->streams.assign(b->branches, nullptr);
-        b->events.assign(b->branches + 1, nullptr);
-        for (auto& s2 : b->streams) AT3R_CUDA(cudaStreamCreateWithFlags(&s2, cudaStreamNonBlocking));
-        for (auto& e : b->events) AT3R_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
-        AT3R_CUDA(cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal));
-        at3r_status rc = AT3R_OK;
-        AT3R_CUDA(cudaEventRecord(b->events[0], cap));
-        for (int k = 0; k < b->branches && !rc; k++)
-            if (cudaStreamWaitEvent(b->streams[k], b->events[0], 0) != cudaSuccess) rc = AT3R_ERR_CUDA;
-        for (size_t i = 0; i < b->plans.size() && !rc; i++)
-            rc = at3r_run_device(b->plans[i], b->proj[i], b->vol[i], b->streams[i % b->branches]);
-        for (int k = 0; k < b->branches && !rc; k++) {
-            if (cudaEventRecord(b->events[k + 1], b->streams[k]) != cudaSuccess ||
-                cudaStreamWaitEvent(cap, b->events[k + 1], 0) != cudaSuccess)
-                rc = AT3R_ERR_CUDA;
+        at3r_status rc;
+        const bool try_waves = b->waves && b->mode_req != AT3R_BATCH_BRANCHES;
+        const bool try_branches = !b->waves || b->mode_req != AT3R_BATCH_WAVES;
+        cudaGraph_t gw = nullptr, gb = nullptr;
+        cudaGraphExec_t xw = nullptr, xb = nullptr;
+        if (try_waves && (rc = capture_batch(b, true, &gw, &xw))) return rc;
+        if (try_branches && (rc = capture_batch(b, false, &gb, &xb))) {
+            if (xw) cudaGraphExecDestroy(xw);
+            if (gw) cudaGraphDestroy(gw);
+            return rc;
         }
-        cudaGraph_t g = nullptr;
-        const cudaError_t ce = cudaStreamEndCapture(cap, &g);
-        cudaStreamDestroy(cap);
-        if (rc || ce != cudaSuccess) {
-            if (g) cudaGraphDestroy(g);
-            cudaGetLastError();
-            return set_err(AT3R_ERR_CUDA, std::string("batch capture failed: ") +
-                                              (rc ? at3r_last_error() : cudaGetErrorString(ce)));
+        b->mode = xw ? AT3R_BATCH_WAVES : AT3R_BATCH_BRANCHES;
+        if (xw && xb) {
+            // both forms were possible: keep the faster on this device
+            float mw = 0.f, mb = 0.f;
+            if ((rc = time_graph(xw, st, &mw)) || (rc = time_graph(xb, st, &mb))) return rc;
+            b->ms_waves = mw;
+            b->ms_branches = mb;
+            b->mode = mw <= mb ? AT3R_BATCH_WAVES : AT3R_BATCH_BRANCHES;
         }
-        b->graph = g;
-        AT3R_CUDA(cudaGraphInstantiate(&b->exec, b->graph, 0));
+        if (b->mode == AT3R_BATCH_WAVES) {
+            b->graph = gw; b->exec = xw;
+            if (xb) { cudaGraphExecDestroy(xb); cudaGraphDestroy(gb); }
+        } else {
+            b->graph = gb; b->exec = xb;
+            if (xw) { cudaGraphExecDestroy(xw); cudaGraphDestroy(gw); }
+        }
     }
     AT3R_CUDA(cudaGraphLaunch(b->exec, st));
     return AT3R_OK;
+}
+
+at3r_status at3r_batch_set_mode(at3r_batch* b, int mode)
+{
+    if (!b || mode < AT3R_BATCH_AUTO || mode > AT3R_BATCH_WAVES)
+        return set_err(AT3R_ERR_INVALID_ARGUMENT, "mode must be AT3R_BATCH_AUTO, _BRANCHES or _WAVES");
+    if (b->exec) return set_err(AT3R_ERR_INVALID_ARGUMENT, "the batch has run already");
+    if (mode == AT3R_BATCH_WAVES && !b->waves)
+        return set_err(AT3R_ERR_UNSUPPORTED, "the wave form needs WBP plans of one storage type");
+    b->mode_req = mode;
+    return AT3R_OK;
+}
+
+int at3r_batch_mode(const at3r_batch* b, float* ms_waves, float* ms_branches)
+{
+    if (!b) return 0;
+    if (ms_waves) *ms_waves = b->ms_waves;
+    if (ms_branches) *ms_branches = b->ms_branches;
+    return b->mode;
 }
 
 void at3r_batch_destroy(at3r_batch* b)
@@ -1582,6 +1907,8 @@ void at3r_batch_destroy(at3r_batch* b)
     if (!b) return;
     if (b->exec) cudaGraphExecDestroy(b->exec);
     if (b->graph) cudaGraphDestroy(b->graph);
+    for (void* ptr : {(void*)b->d_slabs, (void*)b->d_start, (void*)b->d_counters})
+        if (ptr) cudaFree(ptr);
     for (auto s2 : b->streams) if (s2) cudaStreamDestroy(s2);
     for (auto e : b->events) if (e) cudaEventDestroy(e);
     delete b;

@@ -7,6 +7,13 @@
 #include <vector>
 
 extern "C" at3r_status plan_create_impl(const at3r_geom* g, cudaStream_t alloc_stream, at3r_plan** out);
+// Device bytes the serving loop holds for a request (workspace on one lane,
+// FFT tables, the projections resident on the device, two volume slabs);
+// *slab_out (may be null) receives the plan's slab.  0 for invalid sizes.
+size_t at3r_estimate_resident_bytes(const at3r_geom* g, int* slab_out);
+// One slab of a device-resident series proj[T][ny][nx]: rows [y0, y0 + n)
+// into vol_rows[n][Nz][Nx] on `st`, without the per-run bookkeeping.
+at3r_status at3r_plan_run_slab(at3r_plan* p, const float* proj, int y0, int n, float* vol_rows, cudaStream_t st);
 // Sets the calling thread's at3r_last_error() text.
 void at3r_set_last_error(const char* msg);
 // The library's device memory pool of device `dev` (freed blocks stay cached

@@ -219,18 +219,18 @@ __global__ void __launch_bounds__(256) k_gather_weight(const float* __restrict__
 // for the 16-bit row scales).  Grid (ceil(ceil(T/2) / B), slices).
 // ---------------------------------------------------------------------------
 template <typename ST, int RS>
-__global__ void __launch_bounds__(512, RS < 2 ? 2 : 1) k_rweight(const float* __restrict__ proj, size_t tilt_stride, int row_pitch,
+__device__ __forceinline__ void rweight_block(const float* __restrict__ proj, size_t tilt_stride, int row_pitch,
                                                  int y0, const float2* __restrict__ cs, int T, int N, int Nz,
-                                                 const float* __restrict__ hhalf, const __grid_constant__ FftPlan plan, int B,
+                                                 const float* __restrict__ hhalf, const FftPlan& plan, int B,
                                                  ST* __restrict__ out, float* __restrict__ scale,
-                                                 int* __restrict__ flags)
+                                                 int* __restrict__ flags, int bx, int by)
 {
     extern __shared__ float2 fsm[];
     __shared__ float rsc[16];   // per row of the CTA: 1 / scale
     const int pitch = fft_pitch(plan.work);
     float2* a = fsm;
     float2* b = fsm + (size_t)B * pitch;
-    const int ys = blockIdx.y, pair0 = blockIdx.x * B;
+    const int ys = by, pair0 = bx * B;
     const int nq = min(B, (T + 1) / 2 - pair0);   // tilt pairs in this CTA
     const float* srow = proj + (size_t)(y0 + ys) * row_pitch;
     for (int q = 0; q < nq; q++) {
@@ -300,6 +300,16 @@ __global__ void __launch_bounds__(512, RS < 2 ? 2 : 1) k_rweight(const float* __
     if (low) atomicOr(flags + ys, kFlagRawLow);
 }
 
+template <typename ST, int RS>
+__global__ void __launch_bounds__(512, RS < 2 ? 2 : 1) k_rweight(const float* __restrict__ proj, size_t tilt_stride, int row_pitch,
+                                                 int y0, const float2* __restrict__ cs, int T, int N, int Nz,
+                                                 const float* __restrict__ hhalf, const __grid_constant__ FftPlan plan, int B,
+                                                 ST* __restrict__ out, float* __restrict__ scale,
+                                                 int* __restrict__ flags)
+{
+    rweight_block<ST, RS>(proj, tilt_stride, row_pitch, y0, cs, T, N, Nz, hhalf, plan, B, out, scale, flags, blockIdx.x, blockIdx.y);
+}
+
 // ---------------------------------------------------------------------------
 // Back-projection.  MODE 0: SART update on the 1x grid
 // (AreTomo/Recon/GBackProj.cu:12-60, bSart): the mean over tilts [t0, t1) of
@@ -346,6 +356,7 @@ struct BpArgs {
     void* shadow;            // MODE 0, 16-bit volume type: [ceil(slices/8)][GZ][GX] of eight 16-bit values
                              // beside the slice-group volume (shadow_half)
     int* seen;               // run summary: the flags of every slice ORed in (may be null)
+    int bulk;                // FP32 storage: stage window rows by bulk asynchronous copies (bp_smem_bytes(1))
 };
 
 template <int MODE>
@@ -359,9 +370,33 @@ __device__ __forceinline__ float bp_xp(float fX, float fZs, float c, float cent)
     return __fadd_rn(__fmaf_rn(a, 0.5f, cent), 0.5f);
 }
 
-__host__ __device__ inline size_t bp_smem_bytes(int)
+// Raw window rows of the bulk-copy staging: a row is copied from the 16-byte
+// boundary at or below its window start, so it spans at most 3 + 81 floats.
+constexpr int BP_RAW_W = 88;
+constexpr int kFlagStageTimeout = 16;   // a bulk staging wait ran out (the tile was not written)
+
+__host__ __device__ inline size_t bp_smem_bytes(int bulk)
 {
-    return (sizeof(int) + sizeof(float2)) * BP_CHUNK + sizeof(float2) * (size_t)SB * BP_PSLAB;
+    const size_t base = (sizeof(int) + sizeof(float2)) * BP_CHUNK + sizeof(float2) * (size_t)SB * BP_PSLAB;
+    return bulk ? base + 16 + sizeof(float) * (size_t)SB * BP_CHUNK * BP_RAW_W : base;
+}
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// Waits for phase `parity` of the mbarrier at `bar`, at most `limit` polls;
+// false when it gave up.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, int limit)
+{
+    for (int i = 0; i < limit; i++) {
+        uint32_t done;
+        asm volatile(
+            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+            : "=r"(done)
+            : "r"(bar), "r"(parity)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
 }
 
 // Writes one voxel and returns its value afterwards (the old value where no
@@ -459,7 +494,7 @@ __device__ __forceinline__ void bp_store1_grp(const BpArgs& p, int g, int q, int
 // GRP (MODE 0 only): the volume is the slice-group working volume above;
 // otherwise MODE 0 updates a plain [slices][GZ][GX] volume (z flipped).
 template <int MODE, typename ST, typename VT, bool GRP>
-__global__ void __launch_bounds__(BP_THREADS, 3) k_bp(BpArgs p)
+__device__ __forceinline__ void bp_tile(BpArgs p, int bx, int by, int bz)
 {
     static_assert(!GRP || MODE == 0, "the slice-group layout is the SART working volume");
     static_assert(GRP || std::is_same<VT, float>::value, "the 16-bit shadow exists in the slice-group layout only");
@@ -467,8 +502,21 @@ __global__ void __launch_bounds__(BP_THREADS, 3) k_bp(BpArgs p)
     float2* cs_s = bsm;                                               // [BP_CHUNK]
     float2* pw = bsm + BP_CHUNK;                                      // [SB][BP_CHUNK][BP_WW]
     int* ws = reinterpret_cast<int*>(pw + SB * BP_PSLAB);             // [BP_CHUNK]
-    const int ys0 = blockIdx.z * SB, nsl = min(SB, p.S - ys0);
-    const int X0 = blockIdx.x * BP_TX, Z0 = blockIdx.y * BP_TZ;
+    // bulk staging: an mbarrier and the raw rows [SB][BP_CHUNK][BP_RAW_W]
+    uint64_t* mbar = reinterpret_cast<uint64_t*>(ws + BP_CHUNK);
+    float* raw = reinterpret_cast<float*>(reinterpret_cast<char*>(mbar) + 16);
+    const bool bulk = std::is_same<ST, float>::value && p.bulk != 0 && (p.N & 3) == 0;
+    uint32_t phase = 0;
+    bool stage_ok = true;
+    if (bulk) {
+        if (threadIdx.x == 0) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(mbar)) : "memory");
+            asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        }
+        __syncthreads();
+    }
+    const int ys0 = bz * SB, nsl = min(SB, p.S - ys0);
+    const int X0 = bx * BP_TX, Z0 = by * BP_TZ;
     const float cent = MODE == 0 ? (float)p.N / 2.0f : (float)(p.N / 2);
     const float hx = MODE == 0 ? (float)p.GX * 0.5f : (float)p.GX / 2.0f;
     const float hz = MODE == 0 ? (float)p.GZ * 0.5f : (float)p.GZ / 2.0f;
@@ -477,7 +525,7 @@ __global__ void __launch_bounds__(BP_THREADS, 3) k_bp(BpArgs p)
 
     bool low = false;
     for (int q = 0; q < nsl; q++) low |= (__ldg(p.flags + ys0 + q) & p.low_bit) != 0;
-    if (p.seen && blockIdx.x == 0 && blockIdx.y == 0 && (int)threadIdx.x < nsl)
+    if (p.seen && bx == 0 && by == 0 && (int)threadIdx.x < nsl)
         atomicOr(p.seen, __ldg(p.flags + ys0 + threadIdx.x));
 
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -507,6 +555,43 @@ __global__ void __launch_bounds__(BP_THREADS, 3) k_bp(BpArgs p)
             inside = (lo >= 0.01f) && (hi <= endX - 0.01f);
         }
         inside = __syncthreads_and(inside);
+        // bulk staging (FP32): a row whose copy range — from the 16-byte boundary
+        // at or below its window start through the window's last sample, rounded
+        // up to 16 bytes — lies on the detector is fetched by one bulk
+        // asynchronous copy (warp 0, one row per lane, completion counted by
+        // the mbarrier); other rows take the load path below
+        auto bulk_row = [&](int t, int& xa, int& nf) {
+            const int x0 = ws[t];
+            xa = x0 & ~3;
+            nf = (x0 + p.ww + 1 - xa + 3) & ~3;
+            return xa >= 0 && xa + nf <= p.N;
+        };
+        if (bulk && warp == 0) {
+            uint32_t bytes = 0;
+            for (int r = lane; r < ns * nc; r += 32) {
+                int xa, nf;
+                if (bulk_row(r % nc, xa, nf)) bytes += 4u * nf;
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) bytes += __shfl_xor_sync(0xffffffffu, bytes, o);
+            if (lane == 0) {
+                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(mbar)), "r"(bytes)
+                             : "memory");
+            }
+            __syncwarp();
+            for (int r = lane; r < ns * nc; r += 32) {
+                const int q = r / nc, t = r - q * nc;
+                int xa, nf;
+                if (!bulk_row(t, xa, nf)) continue;
+                const float* src = reinterpret_cast<const float*>(p.sino) + ((size_t)(ysA + q) * p.T + c0 + t) * p.N + xa;
+                asm volatile(
+                    "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                        smem_u32(raw + (q * BP_CHUNK + t) * BP_RAW_W)),
+                    "l"(src), "r"(4u * nf), "r"(smem_u32(mbar))
+                    : "memory");
+            }
+        }
         // one warp per (slice, tilt) row, lanes along the window; a lane issues
         // all its loads of the row before its first store, so a warp waits for
         // the L2 once per row rather than once per load
@@ -516,6 +601,14 @@ __global__ void __launch_bounds__(BP_THREADS, 3) k_bp(BpArgs p)
         int q = warp / nc, t = warp - (warp / nc) * nc;
         for (int row = warp; row < ns * nc; row += NW) {
             const int x0 = ws[t];
+            if (bulk) {
+                int xa, nf;
+                if (bulk_row(t, xa, nf)) {
+                    t += NW;
+                    while (t >= nc) { t -= nc; q++; }
+                    continue;
+                }
+            }
             const size_t row_id = (size_t)(ysA + q) * p.T + c0 + t;
             const float sc = std::is_same<ST, float>::value ? 1.f : __ldg(p.scale + row_id);
             const ST* src = reinterpret_cast<const ST*>(p.sino) + row_id * p.N + x0 + lane;
@@ -544,8 +637,30 @@ __global__ void __launch_bounds__(BP_THREADS, 3) k_bp(BpArgs p)
             t += NW;
             while (t >= nc) { t -= nc; q++; }
         }
+        if (bulk) {
+            // every thread waits for the copies (a bounded wait: on timeout the
+            // tile is flagged and left unwritten), then the raw rows become pairs
+            const bool ok = mbar_wait(smem_u32(mbar), phase, 1 << 22);
+            stage_ok = __syncthreads_and(ok && stage_ok) != 0;
+            if (stage_ok) phase ^= 1;
+            for (int e = threadIdx.x; stage_ok && e < ns * nc * p.ww; e += BP_THREADS) {
+                const int r = e / p.ww, k = e - r * p.ww;
+                const int q = r / nc, t = r - q * nc;
+                int xa, nf;
+                if (!bulk_row(t, xa, nf)) continue;
+                const float* rr = raw + (q * BP_CHUNK + t) * BP_RAW_W + (ws[t] - xa) + k;
+                pw[q * BP_PSLAB + t * BP_WW + k] = make_float2(rr[0], rr[1]);
+            }
+        }
         __syncthreads();
         return inside != 0;
+    };
+
+    // a bulk staging wait that ran out: wait once more (bounded) for the
+    // copies still in flight, flag the slab, write nothing
+    auto give_up = [&]() {
+        mbar_wait(smem_u32(mbar), phase, 1 << 22);
+        if (threadIdx.x == 0) atomicOr(p.flags + ys0, kFlagStageTimeout);
     };
 
     if (!low) {
@@ -567,6 +682,7 @@ __global__ void __launch_bounds__(BP_THREADS, 3) k_bp(BpArgs p)
         for (int c0 = p.t0; c0 < p.t1; c0 += BP_CHUNK) {
             const int nc = min(BP_CHUNK, p.t1 - c0);
             const bool inside = stage(c0, nc, ys0, nsl);
+            if (!stage_ok) break;
             if (inside) {
                 // the whole tile lands inside the detector for every tilt of the chunk
                 for (int t = 0; t < nc; t++) {
@@ -624,6 +740,10 @@ __global__ void __launch_bounds__(BP_THREADS, 3) k_bp(BpArgs p)
             }
             __syncthreads();
         }
+        if (!stage_ok) {
+            give_up();
+            return;
+        }
 #pragma unroll
         for (int j = 0; j < BP_CZ; j++) {
             const int Z = Z0 + warp + (BP_THREADS / 32) * j;
@@ -632,7 +752,7 @@ __global__ void __launch_bounds__(BP_THREADS, 3) k_bp(BpArgs p)
                 const int X = X0 + lane + 32 * i;
                 if (Z >= p.GZ || X >= p.GX) continue;
                 if constexpr (GRP) {
-                    bp_store_grp<VT>(p, blockIdx.z, ys0, nsl, Z, X,
+                    bp_store_grp<VT>(p, bz, ys0, nsl, Z, X,
                                      make_float4(sum[0][j][i], sum[1][j][i], sum[2][j][i], sum[3][j][i]), cnt[j][i]);
                 } else {
                     const float k = cnt[j][i] > 0 ? __fdiv_rn(MODE == 0 ? p.relax : 1.f, (float)cnt[j][i]) : 0.f;
@@ -656,6 +776,7 @@ __global__ void __launch_bounds__(BP_THREADS, 3) k_bp(BpArgs p)
         for (int c0 = p.t0; c0 < p.t1; c0 += BP_CHUNK) {
             const int nc = min(BP_CHUNK, p.t1 - c0);
             stage(c0, nc, ys0 + q, 1);
+            if (!stage_ok) break;
             for (int t = 0; t < nc; t++) {
                 const float2 c = cs_s[t];
                 const float2* w = pw + t * BP_WW;
@@ -680,6 +801,10 @@ __global__ void __launch_bounds__(BP_THREADS, 3) k_bp(BpArgs p)
             }
             __syncthreads();
         }
+        if (!stage_ok) {
+            give_up();
+            return;
+        }
 #pragma unroll
         for (int j = 0; j < BP_CZ; j++) {
             const int Z = Z0 + warp + (BP_THREADS / 32) * j;
@@ -688,7 +813,7 @@ __global__ void __launch_bounds__(BP_THREADS, 3) k_bp(BpArgs p)
                 const int X = X0 + lane + 32 * i;
                 if (Z < p.GZ && X < p.GX) {
                     if constexpr (GRP) {
-                        bp_store1_grp<VT>(p, blockIdx.z, q, ys0 + q, Z, X, sum[j][i], cnt[j][i]);
+                        bp_store1_grp<VT>(p, bz, q, ys0 + q, Z, X, sum[j][i], cnt[j][i]);
                     } else {
                         const float k = cnt[j][i] > 0 ? __fdiv_rn(MODE == 0 ? p.relax : 1.f, (float)cnt[j][i]) : 0.f;
                         bp_store<MODE>(p, ys0 + q, Z, X, sum[j][i], cnt[j][i], k);
@@ -697,6 +822,12 @@ __global__ void __launch_bounds__(BP_THREADS, 3) k_bp(BpArgs p)
             }
         }
     }
+}
+
+template <int MODE, typename ST, typename VT, bool GRP>
+__global__ void __launch_bounds__(BP_THREADS, 3) k_bp(BpArgs p)
+{
+    bp_tile<MODE, ST, VT, GRP>(p, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 
 // ---------------------------------------------------------------------------
@@ -1133,15 +1264,15 @@ __global__ void k_fill_table(int* __restrict__ r, int n, unsigned long long seed
 // B row pairs per CTA.  Grid (ceil(Nz / B), slices).
 // ---------------------------------------------------------------------------
 template <int RS>
-__global__ void __launch_bounds__(512, RS < 2 ? 2 : 1) k_row_r2c(const float* __restrict__ g, int Nx, int Nz, const __grid_constant__ FftPlan plan, int B,
-                                                 float2* __restrict__ y)
+__device__ __forceinline__ void row_r2c_block(const float* __restrict__ g, int Nx, int Nz, const FftPlan& plan, int B,
+                                                 float2* __restrict__ y, int bx, int by)
 {
     extern __shared__ float2 fsm[];
     const int pitch = fft_pitch(plan.work);
     float2* a = fsm;
     float2* b = fsm + (size_t)B * pitch;
     const int X2 = 2 * Nx, KX = Nx / 2 + 1;
-    const int pr0 = blockIdx.x * B, ys = blockIdx.y;   // row pairs (2 pr, 2 pr + 1) of the 2Nz rows
+    const int pr0 = bx * B, ys = by;   // row pairs (2 pr, 2 pr + 1) of the 2Nz rows
     const int nq = min(B, Nz - pr0);
     for (int q = 0; q < nq; q++) {
         const float* g0 = g + ((size_t)ys * 2 * Nz + 2 * (pr0 + q)) * X2;
@@ -1163,6 +1294,13 @@ __global__ void __launch_bounds__(512, RS < 2 ? 2 : 1) k_row_r2c(const float* __
     }
 }
 
+template <int RS>
+__global__ void __launch_bounds__(512, RS < 2 ? 2 : 1) k_row_r2c(const float* __restrict__ g, int Nx, int Nz, const __grid_constant__ FftPlan plan, int B,
+                                                 float2* __restrict__ y)
+{
+    row_r2c_block<RS>(g, Nx, Nz, plan, B, y, blockIdx.x, blockIdx.y);
+}
+
 // ---------------------------------------------------------------------------
 // WBP Fourier crop, step 2 (AreTomo/Recon/GBackProjWbp.cu:126-136,
 // MaUtil/GFourierResize2D.cu:7-39): per column kx, forward FFT over the 2Nz
@@ -1172,12 +1310,12 @@ __global__ void __launch_bounds__(512, RS < 2 ? 2 : 1) k_row_r2c(const float* __
 // y: [slices][2Nz][KX] -> w: [slices][Nz][KX].  Grid (ceil(KX/CB), slices).
 // ---------------------------------------------------------------------------
 template <int RS>
-__global__ void __launch_bounds__(512, RS < 2 ? 2 : 1) k_zcrop(const float2* __restrict__ y, int Nx, int Nz, int CB, int pitch,
-                                               const __grid_constant__ FftPlan p2, const __grid_constant__ FftPlan p1, float norm, float2* __restrict__ w)
+__device__ __forceinline__ void zcrop_block(const float2* __restrict__ y, int Nx, int Nz, int CB, int pitch,
+                                               const FftPlan& p2, const FftPlan& p1, float norm, float2* __restrict__ w, int bx, int by)
 {
     extern __shared__ float2 fsm[];
     const int KX = Nx / 2 + 1, Z2 = 2 * Nz;
-    const int kx0 = blockIdx.x * CB, ys = blockIdx.y;
+    const int kx0 = bx * CB, ys = by;
     const int nc = min(CB, KX - kx0);
     float2* a = fsm;
     float2* b = fsm + (size_t)CB * pitch;
@@ -1209,6 +1347,13 @@ __global__ void __launch_bounds__(512, RS < 2 ? 2 : 1) k_zcrop(const float2* __r
     }
 }
 
+template <int RS>
+__global__ void __launch_bounds__(512, RS < 2 ? 2 : 1) k_zcrop(const float2* __restrict__ y, int Nx, int Nz, int CB, int pitch,
+                                               const __grid_constant__ FftPlan p2, const __grid_constant__ FftPlan p1, float norm, float2* __restrict__ w)
+{
+    zcrop_block<RS>(y, Nx, Nz, CB, pitch, p2, p1, norm, w, blockIdx.x, blockIdx.y);
+}
+
 // ---------------------------------------------------------------------------
 // WBP Fourier crop, step 3 (MaUtil/CCufft2D.cpp:108-117, C2R over Nx,
 // unnormalised; MaUtil/CPad2D.cpp:29-39 unpad; AreTomo/Recon/
@@ -1221,15 +1366,15 @@ __global__ void __launch_bounds__(512, RS < 2 ? 2 : 1) k_zcrop(const float2* __r
 // CTA.  Grid (ceil(ceil(Nz/2) / B), slices).
 // ---------------------------------------------------------------------------
 template <int RS>
-__global__ void __launch_bounds__(512, RS < 2 ? 2 : 1) k_x_c2r(const float2* __restrict__ w, int Nx, int Nz, const __grid_constant__ FftPlan plan, int B,
-                                               int packed, float* __restrict__ vol, size_t vol_slice)
+__device__ __forceinline__ void x_c2r_block(const float2* __restrict__ w, int Nx, int Nz, const FftPlan& plan, int B,
+                                               int packed, float* __restrict__ vol, size_t vol_slice, int bx, int by)
 {
     extern __shared__ float2 fsm[];
     const int pitch = fft_pitch(plan.work);
     float2* a = fsm;
     float2* b = fsm + (size_t)B * pitch;
     const int KX = Nx / 2 + 1, H = Nx / 2;
-    const int pz0 = blockIdx.x * B, ys = blockIdx.y;   // z pairs (2 pz, 2 pz + 1)
+    const int pz0 = bx * B, ys = by;   // z pairs (2 pz, 2 pz + 1)
     const int nq = min(B, (Nz + 1) / 2 - pz0);
     for (int q = 0; q < nq; q++) {
         const int z0 = 2 * (pz0 + q);
@@ -1269,6 +1414,95 @@ __global__ void __launch_bounds__(512, RS < 2 ? 2 : 1) k_x_c2r(const float2* __r
             o0[x] = v.x + ((x & 1) ? oa : ea);
             if (two) o0[x - Nx] = v.y + ((x & 1) ? ob : eb);
         }
+    }
+}
+
+template <int RS>
+__global__ void __launch_bounds__(512, RS < 2 ? 2 : 1) k_x_c2r(const float2* __restrict__ w, int Nx, int Nz, const __grid_constant__ FftPlan plan, int B,
+                                               int packed, float* __restrict__ vol, size_t vol_slice)
+{
+    x_c2r_block<RS>(w, Nx, Nz, plan, B, packed, vol, vol_slice, blockIdx.x, blockIdx.y);
+}
+
+// ---------------------------------------------------------------------------
+// Batched WBP: persistent stage kernels over many series.  A wave holds one
+// slab of every series in the batch (series of fewer slabs drop out of later
+// waves); each of the five WBP stages runs as one launch over the whole wave,
+// whose persistent CTAs pull virtual blocks — (series' slab, block of that
+// stage) — from a counter until none is left, and run the same block body
+// the per-series kernels run, so every result is bit-identical to the
+// per-series launches.
+// ---------------------------------------------------------------------------
+struct WbpSlab {
+    const float* proj;        // series projections [T][ny][nx]
+    size_t tilt_stride;
+    int row_pitch, y0;        // nx; first row of the slab
+    const float2* cs;
+    int T, N, Nx, Nz, S;
+    const float* h;           // R-weight transfer function
+    void* filt;               // staged, filtered sinogram (storage type of the batch)
+    float* scale;
+    int* flags;
+    float* g2;                // 2x grid, then the cropped spectrum
+    float2* y;                // row spectra
+    float* vol;               // the slab's first output slice
+    size_t vol_slice;
+    int b_rweight, b_row, b_xc2r, zcrop_cb, zcrop_pitch, packed;
+    float norm;
+    BpArgs bp;
+    FftPlan fN, f2x, f2z, fz, fx;
+    int gx[5];                // virtual grid x of each stage (y is the slab's slices; the BP's y, z below)
+    int bp_gy, bp_gz;
+};
+
+constexpr int kWbpStages = 5;   // rweight, bp, row_r2c, zcrop, x_c2r
+
+// Flags of every slab of the wave to zero (run_slab_t's memset); grid = slabs.
+__global__ void k_wave_flags(const WbpSlab* __restrict__ w)
+{
+    const WbpSlab& d = w[blockIdx.x];
+    for (int i = threadIdx.x; i < d.S; i += blockDim.x) d.flags[i] = 0;
+}
+
+// Stage STAGE of a wave: start[k] is the first virtual block of slab k
+// (start[nslabs] the total); counter starts at 0.
+template <int STAGE, typename ST, int RS>
+__global__ void __launch_bounds__(STAGE == 1 ? BP_THREADS : 512, STAGE == 1 ? 3 : (RS < 2 ? 2 : 1))
+    k_wbp_wave(const WbpSlab* __restrict__ w, const int* __restrict__ start, int nslabs, int* __restrict__ counter)
+{
+    __shared__ int s_item;
+    const int total = start[nslabs];
+    for (;;) {
+        if (threadIdx.x == 0) s_item = atomicAdd(counter, 1);
+        __syncthreads();
+        const int item = s_item;
+        __syncthreads();
+        if (item >= total) return;
+        int lo = 0, hi = nslabs - 1;   // the slab whose block range holds item
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (start[mid] <= item) lo = mid;
+            else hi = mid - 1;
+        }
+        const WbpSlab& d = w[lo];
+        const int v = item - start[lo];
+        const int bx = v % d.gx[STAGE], by = v / d.gx[STAGE];
+        if constexpr (STAGE == 0) {
+            rweight_block<ST, RS>(d.proj, d.tilt_stride, d.row_pitch, d.y0, d.cs, d.T, d.N, d.Nz, d.h, d.fN,
+                                  d.b_rweight, static_cast<ST*>(d.filt), d.scale, d.flags, bx, by);
+        } else if constexpr (STAGE == 1) {
+            bp_tile<1, ST, float, false>(d.bp, bx, by % d.bp_gy, by / d.bp_gy);
+        } else if constexpr (STAGE == 2) {
+            row_r2c_block<RS>(d.g2, d.Nx, d.Nz, d.f2x, d.b_row, d.y, bx, by);
+        } else if constexpr (STAGE == 3) {
+            const float2* yv = d.y;
+            zcrop_block<RS>(yv, d.Nx, d.Nz, d.zcrop_cb, d.zcrop_pitch, d.f2z, d.fz, d.norm,
+                            reinterpret_cast<float2*>(d.g2), bx, by);
+        } else {
+            x_c2r_block<RS>(reinterpret_cast<const float2*>(d.g2), d.Nx, d.Nz, d.fx, d.b_xc2r, d.packed, d.vol,
+                            d.vol_slice, bx, by);
+        }
+        __syncthreads();   // shared memory is reused by the next block
     }
 }
 

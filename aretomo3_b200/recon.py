@@ -128,6 +128,8 @@ _EXPORTS = {
                                       ctypes.c_int, ctypes.c_float]),
     "at3r_plan_flags_seen": (ctypes.c_int, [ctypes.c_void_p]),
     "at3r_plan_fill_table": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t]),
+    "at3r_batch_set_mode": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "at3r_batch_mode": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float)]),
     "at3r_status_str": (ctypes.c_char_p, [ctypes.c_int]),
     "at3r_last_error": (ctypes.c_char_p, []),
 }
@@ -299,9 +301,13 @@ class Plan:
 
 class Batch:
     """Several plans over device-resident series, captured into one CUDA graph
-    (independent series on parallel branches) and replayed as one launch."""
+    and replayed as one launch.  WBP plans of one storage type run as waves of
+    persistent stage kernels across all series (at3r_batch_create); other
+    mixes capture each plan's launches on parallel branches."""
 
-    def __init__(self, plans, proj_ptrs, vol_ptrs, branches: int = 4):
+    MODES = {"auto": 0, "branches": 1, "waves": 2}
+
+    def __init__(self, plans, proj_ptrs, vol_ptrs, branches: int = 4, mode: str = "auto"):
         n = len(plans)
         P = ctypes.c_void_p * n
         self._plans = list(plans)   # keep the plans alive
@@ -309,6 +315,16 @@ class Batch:
         _check(lib().at3r_batch_create(P(*[p._h.value for p in plans]), P(*proj_ptrs), P(*vol_ptrs), n,
                                        int(branches), ctypes.byref(h)))
         self._h = h
+        if mode != "auto":
+            _check(lib().at3r_batch_set_mode(self._h, self.MODES[mode]))
+
+    @property
+    def mode(self):
+        """("branches" | "waves" | None before the first run, ms of the wave
+        form, ms of the branch form) — the timings when the first run chose."""
+        mw, mb = ctypes.c_float(), ctypes.c_float()
+        m = int(lib().at3r_batch_mode(self._h, ctypes.byref(mw), ctypes.byref(mb)))
+        return {0: None, 1: "branches", 2: "waves"}[m], mw.value, mb.value
 
     def run(self, stream: int = 0) -> None:
         _check(lib().at3r_batch_run(self._h, ctypes.c_void_p(stream)))
@@ -337,8 +353,11 @@ class ServerOpts(ctypes.Structure):
 
 class Server:
     """Serving loop on the current device (at3r_server_*): tilt series are
-    submitted as they arrive and reconstructed concurrently, admitted in FIFO
-    order against an HBM budget and a number of in-flight slots."""
+    submitted as they arrive; a request is admitted when its device bytes
+    (plan workspace, its projections held on the device, two volume slabs)
+    fit the HBM budget and fewer than max_inflight requests are active, and
+    the slabs of the active requests interleave on the device (continuous
+    batching at y-slab granularity), each finished slab streamed to host."""
 
     def __init__(self, hbm_budget_bytes: int = 0, max_inflight: int = 4):
         o = ServerOpts(int(hbm_budget_bytes), int(max_inflight))
@@ -347,17 +366,26 @@ class Server:
         self._h = h
         self._keep = {}
 
-    def submit(self, frames: np.ndarray, tilts_deg, vol_z: int, out: np.ndarray | None = None, **kw) -> int:
+    def submit(self, frames: np.ndarray, tilts_deg, vol_z: int, out: np.ndarray | None = None,
+               out_frames=None, **kw) -> int:
         """frames: host float32 [T][ny][nx] (pinned memory overlaps best);
         returns a request id.  The volume lands in `out` (allocated if None),
-        which wait() returns."""
+        which wait() returns; or, with out_frames, in those ny frames of
+        [vol_z][nx & ~1] float32 (they may repeat: a ring that keeps only the
+        last rows written, for timing series whose volume exceeds host memory)."""
         frames = np.ascontiguousarray(frames, dtype=np.float32)
         T, ny, nx = frames.shape
         g, tilts = make_geom(nx, ny, tilts_deg, vol_z, **kw)
-        if out is None:
-            out = np.empty((ny, int(vol_z), nx & ~1), np.float32)
+        if out_frames is not None:
+            if len(out_frames) != ny:
+                raise ValueError("out_frames needs one frame per row")
+            fout = (ctypes.c_void_p * ny)(*[f.ctypes.data for f in out_frames])
+            out = out_frames
+        else:
+            if out is None:
+                out = np.empty((ny, int(vol_z), nx & ~1), np.float32)
+            fout = (ctypes.c_void_p * ny)(*[out[y].ctypes.data for y in range(ny)])
         fin = (ctypes.c_void_p * T)(*[frames[t].ctypes.data for t in range(T)])
-        fout = (ctypes.c_void_p * ny)(*[out[y].ctypes.data for y in range(ny)])
         rid = ctypes.c_int64()
         _check(lib().at3r_server_submit(self._h, ctypes.byref(g), fin, fout, ctypes.byref(rid)))
         self._keep[rid.value] = (frames, out, tilts, fin, fout)

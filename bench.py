@@ -86,6 +86,11 @@ def workload(name: str, seed_offset: int = 0) -> dict:
     elif name == "wbp_4k_rows":
         c = synth.precision_4k(seed=3 + seed_offset)
         c.update(ny=256, method="wbp", label="WBP 4096x256x41 tilts, thickness 1200")
+    elif name == "sart_4k_rows64":
+        # profiling case of the default series: 64 rows (volume 1.26 GB > L2)
+        c = synth.precision_4k(seed=3 + seed_offset)
+        c.update(ny=64, method="sart", relax=0.0,
+                 label="SART 4096x64x41 tilts, thickness 1200, 15 iterations, 5 subsets")
     elif name == "sart_4k":
         c = synth.precision_4k(seed=3 + seed_offset)
         c.update(method="sart", relax=0.0, label="SART 4096x4096x41 tilts, thickness 1200, 15 iterations, 5 subsets")
@@ -499,14 +504,14 @@ def run_our_arm(args, c, rank, world, local_rank):
     clk = m["clocks"]
     sub = {}
     full = rank == 0 and world == 1 and not args.no_cpu_baseline
-    if c.get("with_wbp") and world == 1:
+    if c.get("with_wbp") and world == 1 and not args.primary_only:
         # the metric's WBP half on the same series
         cw = dict(c, method="wbp", name=c["name"] + "_wbp", label=c["wbp_label"])
         w = measure(cw, frames, proj, vol, stream, min(args.steps, 5), 2, min(args.steps, 2), world, gpu_index,
                     clocks=True)
         sub["wbp"] = (cw, w)
     prec = {}
-    if c.get("with_precision") and world == 1:
+    if c.get("with_precision") and world == 1 and not args.primary_only:
         # the reduced-precision form beside the FP32 path, WBP and SART
         for st in ("f16", "bf16"):
             for meth, base in (("sart", (c, m)), ("wbp", sub.get("wbp"))):
@@ -576,7 +581,7 @@ def run_our_arm(args, c, rank, world, local_rank):
                       "working volume in the forward projection; accumulation FP32; bound 1e-3 relative L2 "
                       "against the FP64 oracle")
         line["precision"] = pr
-    if full and c.get("with_reference_cuda"):
+    if full and c.get("with_reference_cuda") and not args.primary_only:
         cw = sub["wbp"][0] if "wbp" in sub else dict(c, method="wbp")
         line["reference_cuda"] = reference_cuda(c, cw, frames)
     print(json.dumps(line), flush=True)
@@ -610,6 +615,7 @@ def run_batch_arm(args):
     clocks = ClockSampler(0)
     clocks.start()
     tot_units, ms_graph, ms_plain, equal, slabs, launches = 0.0, 0.0, 0.0, True, [], 0
+    forms = []
     for g0 in range(0, len(specs), args.group):
         grp = specs[g0:g0 + args.group]
         projs, vols, plans = [], [], []
@@ -651,6 +657,8 @@ def run_batch_arm(args):
         torch.cuda.synchronize()
         ms_graph += e0.elapsed_time(e1)
         equal = equal and all(torch.equal(a, b) for a, b in zip(vols, ref))
+        form, mw, mb = batch.mode
+        forms.append({"form": form, "waves_ms": mw, "branches_ms": mb})
         batch.close()
         for pl in plans:
             pl.close()
@@ -665,12 +673,16 @@ def run_batch_arm(args):
             "data": "synthetic",
             "config": {"workload": f"batched WBP: {len(specs)} seeded series, nx, ny in 512..2048 step 256, "
                                    f"31..61 tilts over +-60 deg, thickness 128..600; groups of {args.group} "
-                                   f"resident series, each group one CUDA-graph launch on {args.branches} branches",
+                                   f"resident series (memory), each group one CUDA-graph launch",
                        "name": "batch_uneven", "storage": args.storage, "series": len(specs),
                        "units_per_step": tot_units,
                        "l2": "inputs larger than L2 (each group holds tens of GB of series and volumes)"},
             "plain_launches": {"value": plain, "unit": UNIT, "ms_per_step": ms_plain / args.steps},
             "speedup_vs_plain": value / plain, "graph_equals_plain": bool(equal),
+            "forms": forms,
+            "forms_note": ("per group, the form the batch's first run kept after timing one graph launch of each: "
+                           "waves = persistent stage kernels over all series, branches = every plan's own "
+                           "launches on parallel branches"),
             "autotuned_slabs": {str(k): slabs.count(k) for k in sorted(set(slabs))},
             "gpu_launches": int(launches), "clocks": clk}
     print(json.dumps(line), flush=True)
@@ -825,6 +837,119 @@ def run_serving_arm(args):
                     "d2h_bytes_per_step": int(np.mean([4 * pool[pi]["ny"] * pool[pi]["vol_z"] * (pool[pi]["nx"] & ~1)
                                                        for pi, _ in reqs]))},
             "error": err, "clocks": clk}
+    print(json.dumps(line), flush=True)
+
+
+def run_serving_4k_arm(args):
+    """Serving at the size of the 4096 x 4096 x 41 series (thickness 1200):
+    args.requests requests, 70 % WBP / 30 % SART 10 iterations 5 subsets, in
+    16-bit storage (args.storage) against the plain FP32 form served one at a
+    time.  Every request reconstructs the seeded series from pinned host
+    frames; its volume rows stream into a pinned ring of 64 frames per
+    request in flight (an 80.5 GB volume per request does not fit host memory
+    twice), so the timing includes every device-to-host copy.  Three
+    arrival patterns: all at once (saturated throughput, the sustainable
+    arrival rate), Poisson at the 20 s acquisition interval accelerated 100x
+    (0.2 s), and Poisson at the real 20 s acquisition interval
+    (args.interarrival_slow, args.requests_slow requests), whose p99 is
+    stated against that interval."""
+    import threading as th
+    import torch
+    from aretomo3_b200 import recon, synth
+    torch.cuda.set_device(0)
+    c = synth.precision_4k(seed=3)
+    frames = torch.from_numpy(synth.make_tilt_series(c["nx"], c["ny"], c["tilts"], c["vol_z"], c["phantom"])) \
+        .pin_memory().numpy()
+    T, ny, nx = frames.shape
+    Nx, Nz = nx & ~1, c["vol_z"]
+    rng = np.random.default_rng(31)
+    n = args.requests
+    kinds = [bool(rng.random() < 0.3) for _ in range(n)]   # True: SART
+    budget = int(args.hbm_budget_gb * (1 << 30))
+    rings = [[f for f in torch.empty((64, Nz, Nx), dtype=torch.float32).pin_memory().numpy()]
+             for _ in range(args.inflight)]
+
+    def run(arrivals, storage, inflight):
+        n = len(arrivals)
+        srv = recon.Server(hbm_budget_bytes=budget, max_inflight=inflight)
+        free = list(range(len(rings)))
+        cv = th.Condition()
+        lat = [None] * n
+        order = []
+        t0 = time.perf_counter()
+
+        def waiter():
+            for k in range(n):
+                with cv:
+                    while k >= len(order):
+                        cv.wait()
+                    rid, i, b, t_sub = order[k]
+                _, l, q = srv.wait(rid)
+                lat[i] = (t_sub - t0 - arrivals[i] + l, q)
+                with cv:
+                    free.append(b)
+                    cv.notify_all()
+
+        w = th.Thread(target=waiter, daemon=True)
+        w.start()
+        for i in range(n):
+            delay = t0 + arrivals[i] - time.perf_counter()
+            if delay > 0:
+                time.sleep(delay)
+            with cv:
+                while not free:
+                    cv.wait()
+                b = free.pop()
+            kw = dict(method=recon.SART, iterations=10, subsets=5) if kinds[i] else dict(method=recon.WBP)
+            ring = rings[b]
+            rid = srv.submit(frames, c["tilts"], Nz, out_frames=[ring[y % 64] for y in range(ny)],
+                             storage=storage, **kw)
+            with cv:
+                order.append((rid, i, b, time.perf_counter()))
+                cv.notify_all()
+        w.join()
+        makespan = time.perf_counter() - t0
+        srv.close()
+        l = np.array([x[0] for x in lat])
+        q = np.array([x[1] for x in lat])
+        return {"p50_s": float(np.percentile(l, 50)), "p99_s": float(np.percentile(l, 99)),
+                "mean_s": float(l.mean()), "max_s": float(l.max()), "queued_p99_s": float(np.percentile(q, 99)),
+                "makespan_s": makespan, "GVoxel_tilt_per_s": n * units_per_step(c) / makespan / 1e9,
+                "series_per_s": n / makespan}
+
+    st16 = STORAGE[args.storage]
+    zeros = np.zeros(n)
+    run(np.zeros(min(n, 2)), st16, args.inflight)   # warm: plans, kernels, FFT convention
+    clocks = ClockSampler(0)
+    clocks.start()
+    served_sat = run(zeros, st16, args.inflight)
+    plain_sat = run(zeros, STORAGE["f32"], 1)
+    fast = rng.exponential(0.2, n)
+    fast = np.cumsum(fast) - fast[0]
+    served_fast = run(fast, st16, args.inflight)
+    n_slow = min(n, args.requests_slow)
+    slow = rng.exponential(args.interarrival_slow, n_slow)
+    slow = np.cumsum(slow) - slow[0]
+    served_slow = run(slow, st16, args.inflight)
+    clk = clocks.stop()
+    sat = served_sat["GVoxel_tilt_per_s"]
+    line = {"metric": METRIC, "value": sat, "unit": UNIT, "n_gpus": 1, "steps": n, "warmup": 2,
+            "ms_per_step": served_sat["makespan_s"] / n * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": f"{args.storage}-storage/f32-accumulate", "data": "synthetic",
+            "config": {"workload": f"serving at 4096x4096x41, thickness 1200: {n} requests, "
+                                   f"{sum(kinds)} SART 10 iterations 5 subsets / {n - sum(kinds)} WBP, "
+                                   f"{args.storage} storage, {args.inflight} requests active, HBM budget "
+                                   f"{args.hbm_budget_gb} GB; pinned host frames in, volume rows streamed into "
+                                   f"pinned rings of 64 frames", "name": "serve_4k", "step": "one request"},
+            "saturated": served_sat, "plain_fp32_one_at_a_time": plain_sat,
+            "speedup_vs_plain_fp32": sat / plain_sat["GVoxel_tilt_per_s"],
+            "sustainable_arrival_per_s": served_sat["series_per_s"],
+            "poisson_0.2s": served_fast,
+            f"poisson_{args.interarrival_slow:g}s": served_slow,
+            "p99_below_acquisition_interval": served_slow["p99_s"] < 20.0,
+            "e2e": {"value": sat, "unit": UNIT, "h2d_bytes_per_step": int(frames.nbytes),
+                    "d2h_bytes_per_step": int(4 * ny * Nz * Nx)},
+            "clocks": clk}
     print(json.dumps(line), flush=True)
 
 
@@ -1026,6 +1151,9 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=3,
                     help="steps of the host-API (e2e) measurement, at most --steps (0: --steps)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--primary-only", action="store_true",
+                    help="the line's own measurement only, without the WBP / precision / reference sub-records "
+                         "(for profiling runs)")
     ap.add_argument("--storage", default="f32", choices=sorted(STORAGE),
                     help="staged-sinogram storage: f32, or f16 / bf16 with per-tilt scale (FP32 accumulation)")
     ap.add_argument("--slab", type=int, default=0, help="slices per device batch (0: the plan's default)")
@@ -1037,6 +1165,10 @@ def main():
     ap.add_argument("--requests", type=int, default=200, help="serve_mix: number of requests")
     ap.add_argument("--pool", type=int, default=16, help="serve_mix: distinct series the requests draw from")
     ap.add_argument("--interarrival", type=float, default=0.2, help="serve_mix: mean Poisson inter-arrival, s")
+    ap.add_argument("--interarrival-slow", type=float, default=20.0,
+                    help="serve_4k: mean Poisson inter-arrival of the run at the acquisition interval, s")
+    ap.add_argument("--requests-slow", type=int, default=6,
+                    help="serve_4k: requests of the run at the acquisition interval")
     ap.add_argument("--inflight", type=int, default=4, help="serve_mix: requests on the GPU at once")
     ap.add_argument("--out-buffers", type=int, default=12, help="serve_mix: pinned host volume buffers")
     ap.add_argument("--hbm-budget-gb", type=float, default=150.0, help="serve_mix: HBM admission budget")
@@ -1053,6 +1185,11 @@ def main():
                                       "d2h_bytes_per_step": 0}}), flush=True)
         else:
             run_stack_arm(args)
+        return
+    if args.impl == "ours" and args.workload == "serve_4k":
+        if args.storage == "f32":
+            args.storage = "f16"
+        run_serving_4k_arm(args)
         return
     if args.impl == "ours" and args.workload in ("batch_uneven", "serve_mix"):
         if args.workload == "batch_uneven":

@@ -137,7 +137,9 @@ int at3r_plan_c2r(const at3r_plan* plan);
  * projection tested every sample and the fill ran; 2 the staged projections
  * held values at or below -5e9 (near the -1e10 "missing" test), so the
  * back-projection tested every sample; 4 the SART residual did; 8 a fill chain
- * found no non-empty voxel and took the slice mean.  -1 on a CUDA error. */
+ * found no non-empty voxel and took the slice mean; 16 a back-projection tile
+ * gave up waiting for its bulk-copy staging (the AT3R_BP_BULK_STAGING=1
+ * option) and was not written.  -1 on a CUDA error. */
 int at3r_plan_flags_seen(const at3r_plan* plan);
 /* The SART plan's fill table (see at3r_geom.fill_seed): Nx * Nz entries, entry
  * i = Z * Nx + X for the voxel at (X, Z) of a slice before the z flip, as
@@ -222,16 +224,32 @@ at3r_status at3r_plan_autotune(at3r_plan* plan, const float* proj, float* vol, v
 /* Slices per device batch the plan currently uses. */
 int at3r_plan_slab(const at3r_plan* plan);
 
-/* Batched form: a fixed set of plans over device-resident series.  The first
- * at3r_batch_run captures every plan's launches into one CUDA graph (plan i
- * on branch i % branches, so independent series overlap on the device) and
- * every run replays it as a single graph launch on `stream`.  Plans, buffers
- * and their contents' sizes must stay as given; SART plans must not compute
- * the R-factor and no plan may have timing enabled. */
+/* Batched form: a fixed set of plans over device-resident series.  When
+ * every plan is WBP with one storage type, the batch runs as waves: wave w
+ * holds slab w of every series that has one, and each of the five WBP
+ * stages (R-weight, 2x-grid back-projection, row FFT, column crop, inverse
+ * rows) is one launch over the whole wave whose persistent CTAs pull blocks
+ * — (series, slab, tile) — from a counter across the uneven series, running
+ * the same block code as the per-series kernels (results bit-identical to
+ * at3r_run_device of each plan).  The branch form captures every plan's own
+ * launches (plan i on branch i % branches).  The first at3r_batch_run
+ * captures the work into one CUDA graph (by default both forms when both are
+ * possible, keeping the one that times faster; at3r_batch_set_mode) and every
+ * run replays it as a single graph launch on `stream`.  Plans, buffers and their
+ * contents' sizes must stay as given; SART plans must not compute the
+ * R-factor and no plan may have timing enabled. */
 typedef struct at3r_batch at3r_batch;
 at3r_status at3r_batch_create(at3r_plan* const* plans, const float* const* proj, float* const* vol, int n,
                               int branches, at3r_batch** out);
+/* Which form the first run captures: AUTO captures both when the wave form
+ * is possible, times one launch of each on the device and keeps the faster;
+ * BRANCHES / WAVES force one (before the first run). */
+enum { AT3R_BATCH_AUTO = 0, AT3R_BATCH_BRANCHES = 1, AT3R_BATCH_WAVES = 2 };
+at3r_status at3r_batch_set_mode(at3r_batch* batch, int mode);
 at3r_status at3r_batch_run(at3r_batch* batch, void* stream);
+/* The form the batch runs (AT3R_BATCH_BRANCHES / _WAVES; 0 before the first
+ * run) and, when AUTO timed both, their device milliseconds (else 0). */
+int at3r_batch_mode(const at3r_batch* batch, float* ms_waves, float* ms_branches);
 void at3r_batch_destroy(at3r_batch* batch);
 
 /* Upper estimate of the device bytes that at3r_plan_create plus one
@@ -240,17 +258,24 @@ void at3r_batch_destroy(at3r_batch* batch);
 size_t at3r_plan_estimate_bytes(const at3r_geom* g);
 
 /* Serving loop (on the current device).  Series are submitted as they are
- * collected and reconstructed concurrently: a request waits in FIFO order
- * until the device bytes it needs fit hbm_budget_bytes beside the running
- * ones and one of max_inflight workers (each with its own stream) is free;
- * its volume streams back slab by slab.  Frames and volume frames are host
- * buffers as for at3r_run_host (pinned memory overlaps best) and must stay
- * valid until at3r_server_wait returns for the request.  Results equal those
- * of a lone at3r_run_host on the same geometry. */
+ * collected and reconstructed concurrently, with continuous batching at
+ * y-slab granularity: a request is admitted as soon as the device bytes it
+ * holds (its plan's workspace, its projections kept on the device for the
+ * whole request, two volume slabs) fit hbm_budget_bytes beside the admitted
+ * ones and fewer than max_inflight requests are active — any queued request
+ * that fits may start, so a large request does not hold back smaller ones,
+ * and one passed over eight times stops further overtaking until it fits.
+ * One engine thread keeps two slabs of every active request queued on that
+ * request's own stream, so slabs of different requests interleave on the
+ * device, and streams each finished slab's volume rows to the host frames.
+ * Frames and volume frames are host buffers as for at3r_run_host (pinned
+ * memory moves directly; pageable memory through pinned bounce buffers) and
+ * must stay valid until at3r_server_wait returns for the request.  Results
+ * equal those of a lone at3r_run_host on the same geometry. */
 typedef struct at3r_server at3r_server;
 typedef struct at3r_server_opts {
     size_t hbm_budget_bytes;   /* 0 = 90% of the device memory free at creation */
-    int max_inflight;          /* 0 = 4 */
+    int max_inflight;          /* requests active at once; 0 = 4 */
 } at3r_server_opts;
 at3r_status at3r_server_create(const at3r_server_opts* opts, at3r_server** out);
 at3r_status at3r_server_submit(at3r_server* server, const at3r_geom* g, const float* const* frames,
