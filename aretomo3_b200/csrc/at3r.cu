@@ -343,9 +343,17 @@ at3r_status run_slab_t(at3r_plan* p, const float* proj, size_t tilt_stride, int 
         a.out = reinterpret_cast<float*>(p->d_w); a.out_slice = (size_t)Nx * Nz; a.ww = p->bp_ww_sart;
         a.flags = p->d_flags; a.seen = p->d_seen; a.bulk = p->bp_bulk;
         a.scale = p->d_scale; a.shadow = p->d_shadow;
-        const dim3 bgrid((Nx + BP_TX - 1) / BP_TX, (Nz + BP_TZ - 1) / BP_TZ, SG);
+        const dim3 bgrid = bp_paired<VT>()
+                               ? dim3(2 * ((Nx + BP_TX - 1) / BP_TX), (Nz + BP_TZ - 1) / BP_TZ, (SG + 1) / 2)
+                               : dim3((Nx + BP_TX - 1) / BP_TX, (Nz + BP_TZ - 1) / BP_TZ, SG);
         auto bp_launch = [&](int nt_) {
-            k_bp<0, ST, VT, true><<<bgrid, BP_THREADS, bp_smem(a.bulk), st>>>(a);
+            if constexpr (std::is_same<ST, float>::value) {
+                if (a.bulk) {
+                    k_bp<0, ST, VT, true, true><<<bgrid, BP_THREADS, bp_smem(1), st>>>(a);
+                    return;
+                }
+            }
+            k_bp<0, ST, VT, true><<<bgrid, BP_THREADS, bp_smem(0), st>>>(a);
         };
         // first back-projection: all tilts, relax 1 (CTomoSart.cpp:68-69)
         a.sino = raw; a.t0 = 0; a.t1 = T; a.relax = 1.f; a.low_bit = kFlagRawLow;
@@ -400,8 +408,15 @@ at3r_status run_slab_t(at3r_plan* p, const float* proj, size_t tilt_stride, int 
     a.GX = 2 * Nx; a.GZ = 2 * Nz; a.S = S; a.relax = 1.f; a.out = g2; a.out_slice = (size_t)4 * Nx * Nz;
     a.ww = p->bp_ww_wbp; a.flags = flags; a.seen = p->d_seen; a.low_bit = kFlagRawLow; a.bulk = p->bp_bulk;
     TB(p, st);
-    k_bp<1, ST, float, false><<<dim3((2 * Nx + BP_TX - 1) / BP_TX, (2 * Nz + BP_TZ - 1) / BP_TZ, SG), BP_THREADS,
-                                bp_smem(a.bulk), st>>>(a);
+    const dim3 wgrid((2 * Nx + BP_TX - 1) / BP_TX, (2 * Nz + BP_TZ - 1) / BP_TZ, SG);
+    bool launched = false;
+    if constexpr (std::is_same<ST, float>::value) {
+        if (a.bulk) {
+            k_bp<1, ST, float, false, true><<<wgrid, BP_THREADS, bp_smem(1), st>>>(a);
+            launched = true;
+        }
+    }
+    if (!launched) k_bp<1, ST, float, false><<<wgrid, BP_THREADS, bp_smem(0), st>>>(a);
     TE(p, st, KK_BP_WBP, es * S * (double)T * N + f4 * 4 * vox, 4 * vox * T);
     TB(p, st);
     dispatch_rs(p->f2x.rs, [&](auto R) {
@@ -625,7 +640,7 @@ at3r_status plan_create_impl(const at3r_geom* g, cudaStream_t alloc_stream, at3r
     p->g.tilts_deg = p->tilts.data();
     p->nx = g->nx; p->ny = g->ny; p->T = g->n_tilts;
     p->fill_seed = g->fill_seed;
-    p->bp_bulk = g->storage == AT3R_STORE_F32 && bp_bulk_from_env() ? 1 : 0;
+    p->bp_bulk = g->storage == AT3R_STORE_F32 && (g->nx & 3) == 0 && bp_bulk_from_env() ? 1 : 0;
     p->N = g->nx & ~1; p->Nx = p->N; p->Nz = g->vol_z; p->KX = p->Nx / 2 + 1;
     cudaGetDevice(&p->device);
 
@@ -663,7 +678,8 @@ at3r_status plan_create_impl(const at3r_geom* g, cudaStream_t alloc_stream, at3r
         if (p->bp_ww_sart > BP_WW) return fail(set_err(AT3R_ERR_TOO_LARGE, "back-projection window exceeds its stride"));
         for (const void* fn : {(const void*)k_bp<0, float, float, true>, (const void*)k_bp<0, __half, __half, true>,
                                (const void*)k_bp<0, __nv_bfloat16, __nv_bfloat16, true>})
-            if ((rc = set_smem(fn, bp_smem(p->bp_bulk)))) return fail(rc);
+            if ((rc = set_smem(fn, bp_smem(0)))) return fail(rc);
+        if (p->bp_bulk && (rc = set_smem((const void*)k_bp<0, float, float, true, true>, bp_smem(1)))) return fail(rc);
         per_slice = 2 * T * N * p->esz + 4 * Nx * Nz + (p->esz < 4 ? 2 * Nx * Nz + 4 * T : 0);
     } else {
         if (g->c2r == AT3R_C2R_MATCH_CUFFT) {
@@ -717,7 +733,8 @@ at3r_status plan_create_impl(const at3r_geom* g, cudaStream_t alloc_stream, at3r
             if ((rc = set_smem(f.first, f.second))) return fail(rc);
         for (const void* fn : {(const void*)k_bp<1, float, float, false>, (const void*)k_bp<1, __half, float, false>,
                                (const void*)k_bp<1, __nv_bfloat16, float, false>})
-            if ((rc = set_smem(fn, bp_smem(p->bp_bulk)))) return fail(rc);
+            if ((rc = set_smem(fn, bp_smem(0)))) return fail(rc);
+        if (p->bp_bulk && (rc = set_smem((const void*)k_bp<1, float, float, false, true>, bp_smem(1)))) return fail(rc);
         // R-weight transfer function (GRWeight.cu:15-20), 1/N folded in
         std::vector<float> h(N / 2 + 1);
         const double twopi = (double)6.2831852f;

@@ -140,6 +140,16 @@ __device__ __forceinline__ float add_f32_f16(float acc, __half h)
     return r;
 }
 
+// a * b + c with FP16 a, b and an FP32 c and result, one instruction; the
+// product of two FP16 values is exact in FP32, so this is fma(float(a),
+// float(b), c).
+__device__ __forceinline__ float fma_f32_f16(__half a, __half b, float c)
+{
+    float r;
+    asm("fma.rn.f32.f16 %0, %1, %2, %3;" : "=f"(r) : "h"(__half_as_ushort(a)), "h"(__half_as_ushort(b)), "f"(c));
+    return r;
+}
+
 __device__ __forceinline__ float comp(const float4& v, int q)
 {
     return q == 0 ? v.x : q == 1 ? v.y : q == 2 ? v.z : v.w;
@@ -356,7 +366,7 @@ struct BpArgs {
     void* shadow;            // MODE 0, 16-bit volume type: [ceil(slices/8)][GZ][GX] of eight 16-bit values
                              // beside the slice-group volume (shadow_half)
     int* seen;               // run summary: the flags of every slice ORed in (may be null)
-    int bulk;                // FP32 storage: stage window rows by bulk asynchronous copies (bp_smem_bytes(1))
+    int bulk;                // FP32 storage, N % 4 == 0: launch the bulk-copy staging form (bp_smem_bytes(1))
 };
 
 template <int MODE>
@@ -493,9 +503,15 @@ __device__ __forceinline__ void bp_store1_grp(const BpArgs& p, int g, int q, int
 
 // GRP (MODE 0 only): the volume is the slice-group working volume above;
 // otherwise MODE 0 updates a plain [slices][GZ][GX] volume (z flipped).
-template <int MODE, typename ST, typename VT, bool GRP>
+// BULK (FP32 storage, N a multiple of 4): window rows staged by bulk
+// asynchronous copies, the comparison form; the default form has none of its code.
+template <int MODE, typename ST, typename VT, bool GRP, bool BULK = false>
 __device__ __forceinline__ void bp_tile(BpArgs p, int bx, int by, int bz)
 {
+    // FP16 WBP (MODE 1) stages FP16 values and differences (below); SART keeps
+    // the FP32 pairs, where the per-sample conversion of the fraction to FP16
+    // cost more than the halved shared-memory bytes saved
+    constexpr bool H2 = std::is_same<ST, __half>::value && MODE == 1;
     static_assert(!GRP || MODE == 0, "the slice-group layout is the SART working volume");
     static_assert(GRP || std::is_same<VT, float>::value, "the 16-bit shadow exists in the slice-group layout only");
     extern __shared__ float2 bsm[];
@@ -505,7 +521,7 @@ __device__ __forceinline__ void bp_tile(BpArgs p, int bx, int by, int bz)
     // bulk staging: an mbarrier and the raw rows [SB][BP_CHUNK][BP_RAW_W]
     uint64_t* mbar = reinterpret_cast<uint64_t*>(ws + BP_CHUNK);
     float* raw = reinterpret_cast<float*>(reinterpret_cast<char*>(mbar) + 16);
-    const bool bulk = std::is_same<ST, float>::value && p.bulk != 0 && (p.N & 3) == 0;
+    constexpr bool bulk = BULK && std::is_same<ST, float>::value;
     uint32_t phase = 0;
     bool stage_ok = true;
     if (bulk) {
@@ -529,6 +545,25 @@ __device__ __forceinline__ void bp_tile(BpArgs p, int bx, int by, int bz)
         atomicOr(p.seen, __ldg(p.flags + ys0 + threadIdx.x));
 
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    // H2: the fast path stages each window position as FP16 values and
+    // differences in a common scale per slice (the largest row scale of the
+    // launch's tilts), so a sample interpolates two slices per fma.f16x2
+    __shared__ float ssc[SB];
+    __shared__ float rq[SB][BP_CHUNK];
+    float slice_scale[SB];
+    if constexpr (H2) {
+        if (warp < SB) {
+            float m = 0.f;
+            if (warp < nsl)
+                for (int t = p.t0 + lane; t < p.t1; t += 32) m = fmaxf(m, __ldg(p.scale + (size_t)(ys0 + warp) * p.T + t));
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+            if (lane == 0) ssc[warp] = m > 0.f ? m : 1.f;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int q = 0; q < SB; q++) slice_scale[q] = ssc[q];
+    }
     float fX[BP_CX], fZ[BP_CZ];
 #pragma unroll
     for (int i = 0; i < BP_CX; i++) fX[i] = (float)(X0 + lane + 32 * i) - hx;
@@ -537,8 +572,14 @@ __device__ __forceinline__ void bp_tile(BpArgs p, int bx, int by, int bz)
 
     // stage chunk [c0, c0 + nc) of slices [ys0, ys0 + ns) into pw; returns
     // whether the whole tile stays strictly inside the detector for it
-    auto stage = [&](int c0, int nc, int ysA, int ns) -> bool {
+    auto stage = [&](int c0, int nc, int ysA, int ns, bool h2) -> bool {
         int inside = 1;
+        if (H2 && h2 && threadIdx.x < nc) {
+#pragma unroll
+            for (int q = 0; q < SB; q++)
+                rq[q][threadIdx.x] =
+                    q < ns ? __fdiv_rn(__ldg(p.scale + (size_t)(ysA + q) * p.T + c0 + threadIdx.x), ssc[q]) : 0.f;
+        }
         if (threadIdx.x < nc) {
             const float2 c = __ldg(&p.cs[c0 + threadIdx.x]);
             float lo = 3.0e38f, hi = -3.0e38f;
@@ -555,6 +596,45 @@ __device__ __forceinline__ void bp_tile(BpArgs p, int bx, int by, int bz)
             inside = (lo >= 0.01f) && (hi <= endX - 0.01f);
         }
         inside = __syncthreads_and(inside);
+        if constexpr (H2) {
+            if (h2) {
+                // entry (t, k) = {v0 v1, v2 v3, d0 d1, d2 d3} (FP16): v_q the value of
+                // slice q at window position k, d_q = v_q(k + 1) - v_q(k), both in
+                // units of the slice's scale; slices past the slab stay zero.  One
+                // warp per tilt, lanes along the window.  (No value here is a
+                // missing-value marker: a row holding one flags its slice, which
+                // takes the per-slice path.)
+                uint4* ph = reinterpret_cast<uint4*>(pw);
+                constexpr int NW = BP_THREADS / 32;
+                for (int t = warp; t < nc; t += NW) {
+                    const int x0 = ws[t];
+                    const bool on = x0 >= 0 && x0 + p.ww + 1 <= p.N;   // warp-uniform
+                    for (int k = lane; k < p.ww; k += 32) {
+                        const int x = x0 + k;
+                        float v[SB], d[SB];
+#pragma unroll
+                        for (int q = 0; q < SB; q++) {
+                            float a = 0.f, b = 0.f;
+                            if (q < ns) {
+                                const __half* src =
+                                    reinterpret_cast<const __half*>(p.sino) + ((size_t)(ysA + q) * p.T + c0 + t) * p.N;
+                                if (on || (x >= 0 && x < p.N)) a = __half2float(__ldg(src + x));
+                                if (on || (x + 1 >= 0 && x + 1 < p.N)) b = __half2float(__ldg(src + x + 1));
+                            }
+                            const float r = rq[q][t];
+                            v[q] = __fmul_rn(a, r);
+                            d[q] = __fmul_rn(__fsub_rn(b, a), r);
+                        }
+                        ph[t * BP_WW + k] = make_uint4(bits_of(__floats2half2_rn(v[0], v[1])),
+                                                       bits_of(__floats2half2_rn(v[2], v[3])),
+                                                       bits_of(__floats2half2_rn(d[0], d[1])),
+                                                       bits_of(__floats2half2_rn(d[2], d[3])));
+                    }
+                }
+                __syncthreads();
+                return inside != 0;
+            }
+        }
         // bulk staging (FP32): a row whose copy range — from the 16-byte boundary
         // at or below its window start through the window's last sample, rounded
         // up to 16 bytes — lies on the detector is fetched by one bulk
@@ -664,7 +744,7 @@ __device__ __forceinline__ void bp_tile(BpArgs p, int bx, int by, int bz)
     };
 
     if (!low) {
-        if (GRP && nsl < SB) {
+        if (!H2 && GRP && nsl < SB) {
             // rows of slices past the slab's end stay zero (staging never writes them)
             for (int k = threadIdx.x; k < (SB - nsl) * BP_PSLAB; k += BP_THREADS)
                 pw[nsl * BP_PSLAB + k] = make_float2(0.f, 0.f);
@@ -681,9 +761,66 @@ __device__ __forceinline__ void bp_tile(BpArgs p, int bx, int by, int bz)
             }
         for (int c0 = p.t0; c0 < p.t1; c0 += BP_CHUNK) {
             const int nc = min(BP_CHUNK, p.t1 - c0);
-            const bool inside = stage(c0, nc, ys0, nsl);
+            const bool inside = stage(c0, nc, ys0, nsl, true);
             if (!stage_ok) break;
-            if (inside) {
+            if (H2 && inside) {
+                const uint4* ph = reinterpret_cast<const uint4*>(pw);
+                for (int t = 0; t < nc; t++) {
+                    const float2 c = cs_s[t];
+                    const int wb = t * BP_WW - ws[t] - kMagicBits;
+#pragma unroll
+                    for (int j = 0; j < BP_CZ; j++) {
+                        const float fzs = __fmul_rn(fZ[j], c.y);
+#pragma unroll
+                        for (int i = 0; i < BP_CX; i++) {
+                            const float xp = bp_xp<MODE>(fX[i], fzs, c.x, cent);
+                            const float tr = __fadd_rd(xp, kMagic);
+                            const float fr = __fsub_rn(xp, __fsub_rn(tr, kMagic));
+                            const uint4 e = ph[__float_as_int(tr) + wb];
+                            const __half2 f2 = __float2half2_rn(fr);
+                            const __half2 v01 = __hfma2(from_bits<__half2>(e.z), f2, from_bits<__half2>(e.x));
+                            const __half2 v23 = __hfma2(from_bits<__half2>(e.w), f2, from_bits<__half2>(e.y));
+                            sum[0][j][i] = add_f32_f16(sum[0][j][i], __low2half(v01));
+                            sum[1][j][i] = add_f32_f16(sum[1][j][i], __high2half(v01));
+                            sum[2][j][i] = add_f32_f16(sum[2][j][i], __low2half(v23));
+                            sum[3][j][i] = add_f32_f16(sum[3][j][i], __high2half(v23));
+                        }
+                    }
+                }
+#pragma unroll
+                for (int j = 0; j < BP_CZ; j++)
+#pragma unroll
+                    for (int i = 0; i < BP_CX; i++) cnt[j][i] += nc;
+            } else if (H2) {
+                const uint4* ph = reinterpret_cast<const uint4*>(pw);
+                for (int t = 0; t < nc; t++) {
+                    const float2 c = cs_s[t];
+                    const uint4* w = ph + t * BP_WW;
+                    const int st = ws[t];
+#pragma unroll
+                    for (int j = 0; j < BP_CZ; j++) {
+                        const float fzs = __fmul_rn(fZ[j], c.y);
+#pragma unroll
+                        for (int i = 0; i < BP_CX; i++) {
+                            const float xp = bp_xp<MODE>(fX[i], fzs, c.x, cent);
+                            const bool in = xp >= 0.f && xp <= endX;
+                            const int ii = (int)xp;
+                            const float fr = __fsub_rn(xp, (float)ii);
+                            const uint4 e = w[min((unsigned)(ii - st), wmax)];
+                            const __half2 f2 = __float2half2_rn(fr);
+                            const __half2 v01 = __hfma2(from_bits<__half2>(e.z), f2, from_bits<__half2>(e.x));
+                            const __half2 v23 = __hfma2(from_bits<__half2>(e.w), f2, from_bits<__half2>(e.y));
+                            if (in) {
+                                sum[0][j][i] = add_f32_f16(sum[0][j][i], __low2half(v01));
+                                sum[1][j][i] = add_f32_f16(sum[1][j][i], __high2half(v01));
+                                sum[2][j][i] = add_f32_f16(sum[2][j][i], __low2half(v23));
+                                sum[3][j][i] = add_f32_f16(sum[3][j][i], __high2half(v23));
+                                cnt[j][i] += 1;
+                            }
+                        }
+                    }
+                }
+            } else if (inside) {
                 // the whole tile lands inside the detector for every tilt of the chunk
                 for (int t = 0; t < nc; t++) {
                     const float2 c = cs_s[t];
@@ -751,6 +888,10 @@ __device__ __forceinline__ void bp_tile(BpArgs p, int bx, int by, int bz)
             for (int i = 0; i < BP_CX; i++) {
                 const int X = X0 + lane + 32 * i;
                 if (Z >= p.GZ || X >= p.GX) continue;
+                if constexpr (H2) {
+#pragma unroll
+                    for (int q = 0; q < SB; q++) sum[q][j][i] = __fmul_rn(sum[q][j][i], slice_scale[q]);
+                }
                 if constexpr (GRP) {
                     bp_store_grp<VT>(p, bz, ys0, nsl, Z, X,
                                      make_float4(sum[0][j][i], sum[1][j][i], sum[2][j][i], sum[3][j][i]), cnt[j][i]);
@@ -775,7 +916,7 @@ __device__ __forceinline__ void bp_tile(BpArgs p, int bx, int by, int bz)
             for (int i = 0; i < BP_CX; i++) { sum[j][i] = 0.f; cnt[j][i] = 0; }
         for (int c0 = p.t0; c0 < p.t1; c0 += BP_CHUNK) {
             const int nc = min(BP_CHUNK, p.t1 - c0);
-            stage(c0, nc, ys0 + q, 1);
+            stage(c0, nc, ys0 + q, 1, false);
             if (!stage_ok) break;
             for (int t = 0; t < nc; t++) {
                 const float2 c = cs_s[t];
@@ -824,10 +965,24 @@ __device__ __forceinline__ void bp_tile(BpArgs p, int bx, int by, int bz)
     }
 }
 
-template <int MODE, typename ST, typename VT, bool GRP>
+// Grid (tiles x, tiles z, slice groups).  With a 16-bit shadow the two slice
+// groups that share its 16-byte elements run as neighbouring CTAs instead —
+// grid (2 * tiles x, tiles z, ceil(groups / 2)), the group's low bit fastest
+// (k_bp_grid) — so both halves of an element reach L2 together and leave it
+// as whole sectors.
+template <typename VT>
+__host__ __device__ constexpr bool bp_paired() { return !std::is_same<VT, float>::value; }
+
+template <int MODE, typename ST, typename VT, bool GRP, bool BULK = false>
 __global__ void __launch_bounds__(BP_THREADS, 3) k_bp(BpArgs p)
 {
-    bp_tile<MODE, ST, VT, GRP>(p, blockIdx.x, blockIdx.y, blockIdx.z);
+    if constexpr (GRP && bp_paired<VT>()) {
+        const int g = 2 * (int)blockIdx.z + (int)(blockIdx.x & 1);
+        if (g * SB >= p.S) return;
+        bp_tile<MODE, ST, VT, GRP, BULK>(p, blockIdx.x >> 1, blockIdx.y, g);
+    } else {
+        bp_tile<MODE, ST, VT, GRP, BULK>(p, blockIdx.x, blockIdx.y, blockIdx.z);
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -924,7 +1079,7 @@ __device__ __forceinline__ float bf_hi(uint32_t u) { return __uint_as_float(u & 
 // eight); otherwise (FP32 only) the volume is plain [slices][Nz][Nx].
 // Grid (ceil(N/256), tilts, ceil(slices / fp_slices<VT>())).
 template <typename ST, typename VT, bool GRP>
-__global__ void __launch_bounds__(256) k_fp_diff(const float* __restrict__ vol, const void* __restrict__ shadow,
+__global__ void __launch_bounds__(256, std::is_same<VT, float>::value ? 6 : 1) k_fp_diff(const float* __restrict__ vol, const void* __restrict__ shadow,
                                                  int Nx, int Nz, int S, const ST* __restrict__ raw,
                                                  ST* __restrict__ diff, const float* __restrict__ scale,
                                                  const float2* __restrict__ cs, int T, int N, int t0,
@@ -994,18 +1149,27 @@ __global__ void __launch_bounds__(256) k_fp_diff(const float* __restrict__ vol, 
                 const uint32_t p00[4] = {b00.x, b00.y, b00.z, b00.w}, p10[4] = {b10.x, b10.y, b10.z, b10.w};
                 const uint32_t p01[4] = {b01.x, b01.y, b01.z, b01.w}, p11[4] = {b11.x, b11.y, b11.z, b11.w};
                 if constexpr (std::is_same<VT, __half>::value) {
-                    // the sample value of two slices per half2 instruction,
-                    // added to the FP32 sums by mixed-precision adds
-                    const __half2 h00 = __float2half2_rn(w00), h10 = __float2half2_rn(w10);
-                    const __half2 h01 = __float2half2_rn(w01), h11 = __float2half2_rn(w11);
+                    // FP16 weights (two per conversion) times FP16 taps, summed in
+                    // FP32 by mixed-precision fused multiply-adds (full rate on
+                    // B200, where f16x2 arithmetic issues at half rate)
+                    const __half2 wa = __floats2half2_rn(w00, w10), wb = __floats2half2_rn(w01, w11);
+                    const __half w00h = __low2half(wa), w10h = __high2half(wa);
+                    const __half w01h = __low2half(wb), w11h = __high2half(wb);
 #pragma unroll
                     for (int k = 0; k < 4; k++) {
-                        __half2 v = __hmul2(h00, from_bits<__half2>(p00[k]));
-                        v = __hfma2(h10, from_bits<__half2>(p10[k]), v);
-                        v = __hfma2(h01, from_bits<__half2>(p01[k]), v);
-                        v = __hfma2(h11, from_bits<__half2>(p11[k]), v);
-                        fSum[2 * k] = add_f32_f16(fSum[2 * k], __low2half(v));
-                        fSum[2 * k + 1] = add_f32_f16(fSum[2 * k + 1], __high2half(v));
+                        const __half2 a00 = from_bits<__half2>(p00[k]), a10 = from_bits<__half2>(p10[k]);
+                        const __half2 a01 = from_bits<__half2>(p01[k]), a11 = from_bits<__half2>(p11[k]);
+                        float s0 = fSum[2 * k], s1 = fSum[2 * k + 1];
+                        s0 = fma_f32_f16(w00h, __low2half(a00), s0);
+                        s1 = fma_f32_f16(w00h, __high2half(a00), s1);
+                        s0 = fma_f32_f16(w10h, __low2half(a10), s0);
+                        s1 = fma_f32_f16(w10h, __high2half(a10), s1);
+                        s0 = fma_f32_f16(w01h, __low2half(a01), s0);
+                        s1 = fma_f32_f16(w01h, __high2half(a01), s1);
+                        s0 = fma_f32_f16(w11h, __low2half(a11), s0);
+                        s1 = fma_f32_f16(w11h, __high2half(a11), s1);
+                        fSum[2 * k] = s0;
+                        fSum[2 * k + 1] = s1;
                     }
                 } else {
 #pragma unroll
