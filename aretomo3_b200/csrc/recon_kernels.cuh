@@ -140,16 +140,6 @@ __device__ __forceinline__ float add_f32_f16(float acc, __half h)
     return r;
 }
 
-// a * b + c with FP16 a, b and an FP32 c and result, one instruction; the
-// product of two FP16 values is exact in FP32, so this is fma(float(a),
-// float(b), c).
-__device__ __forceinline__ float fma_f32_f16(__half a, __half b, float c)
-{
-    float r;
-    asm("fma.rn.f32.f16 %0, %1, %2, %3;" : "=f"(r) : "h"(__half_as_ushort(a)), "h"(__half_as_ushort(b)), "f"(c));
-    return r;
-}
-
 __device__ __forceinline__ float comp(const float4& v, int q)
 {
     return q == 0 ? v.x : q == 1 ? v.y : q == 2 ? v.z : v.w;
@@ -546,8 +536,8 @@ __device__ __forceinline__ void bp_tile(BpArgs p, int bx, int by, int bz)
 
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     // H2: the fast path stages each window position as FP16 values and
-    // differences in a common scale per slice (the largest row scale of the
-    // launch's tilts), so a sample interpolates two slices per fma.f16x2
+    // differences in a common scale per slice (2^-12 of the largest row scale
+    // of the launch's tilts), so a sample interpolates two slices per fma.f16x2
     __shared__ float ssc[SB];
     __shared__ float rq[SB][BP_CHUNK];
     float slice_scale[SB];
@@ -558,7 +548,10 @@ __device__ __forceinline__ void bp_tile(BpArgs p, int bx, int by, int bz)
                 for (int t = p.t0 + lane; t < p.t1; t += 32) m = fmaxf(m, __ldg(p.scale + (size_t)(ys0 + warp) * p.T + t));
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
-            if (lane == 0) ssc[warp] = m > 0.f ? m : 1.f;
+            // 2^-12 of the largest row scale: the largest values stage as up to
+            // 4096 (FP16 holds 65504), and rows far weaker than the strongest
+            // stay above FP16's subnormal range
+            if (lane == 0) ssc[warp] = m > 0.f ? m * 0x1p-12f : 1.f;
         }
         __syncthreads();
 #pragma unroll
@@ -1149,27 +1142,18 @@ __global__ void __launch_bounds__(256, std::is_same<VT, float>::value ? 6 : 1) k
                 const uint32_t p00[4] = {b00.x, b00.y, b00.z, b00.w}, p10[4] = {b10.x, b10.y, b10.z, b10.w};
                 const uint32_t p01[4] = {b01.x, b01.y, b01.z, b01.w}, p11[4] = {b11.x, b11.y, b11.z, b11.w};
                 if constexpr (std::is_same<VT, __half>::value) {
-                    // FP16 weights (two per conversion) times FP16 taps, summed in
-                    // FP32 by mixed-precision fused multiply-adds (full rate on
-                    // B200, where f16x2 arithmetic issues at half rate)
-                    const __half2 wa = __floats2half2_rn(w00, w10), wb = __floats2half2_rn(w01, w11);
-                    const __half w00h = __low2half(wa), w10h = __high2half(wa);
-                    const __half w01h = __low2half(wb), w11h = __high2half(wb);
+                    // the sample value of two slices per half2 instruction,
+                    // added to the FP32 sums by mixed-precision adds
+                    const __half2 h00 = __float2half2_rn(w00), h10 = __float2half2_rn(w10);
+                    const __half2 h01 = __float2half2_rn(w01), h11 = __float2half2_rn(w11);
 #pragma unroll
                     for (int k = 0; k < 4; k++) {
-                        const __half2 a00 = from_bits<__half2>(p00[k]), a10 = from_bits<__half2>(p10[k]);
-                        const __half2 a01 = from_bits<__half2>(p01[k]), a11 = from_bits<__half2>(p11[k]);
-                        float s0 = fSum[2 * k], s1 = fSum[2 * k + 1];
-                        s0 = fma_f32_f16(w00h, __low2half(a00), s0);
-                        s1 = fma_f32_f16(w00h, __high2half(a00), s1);
-                        s0 = fma_f32_f16(w10h, __low2half(a10), s0);
-                        s1 = fma_f32_f16(w10h, __high2half(a10), s1);
-                        s0 = fma_f32_f16(w01h, __low2half(a01), s0);
-                        s1 = fma_f32_f16(w01h, __high2half(a01), s1);
-                        s0 = fma_f32_f16(w11h, __low2half(a11), s0);
-                        s1 = fma_f32_f16(w11h, __high2half(a11), s1);
-                        fSum[2 * k] = s0;
-                        fSum[2 * k + 1] = s1;
+                        __half2 v = __hmul2(h00, from_bits<__half2>(p00[k]));
+                        v = __hfma2(h10, from_bits<__half2>(p10[k]), v);
+                        v = __hfma2(h01, from_bits<__half2>(p01[k]), v);
+                        v = __hfma2(h11, from_bits<__half2>(p11[k]), v);
+                        fSum[2 * k] = add_f32_f16(fSum[2 * k], __low2half(v));
+                        fSum[2 * k + 1] = add_f32_f16(fSum[2 * k + 1], __high2half(v));
                     }
                 } else {
 #pragma unroll
