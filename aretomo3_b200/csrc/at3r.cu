@@ -236,6 +236,14 @@ bool bp_bulk_from_env()
     return e && e[0] == '1';
 }
 
+// Threads of a row / column FFT launch: 1024 when two CTAs' shared memory
+// would not fit one SM (so one CTA holds 32 warps) and the radix set allows.
+int fft_threads(int rs, size_t smem)
+{
+    const bool one_cta = 2 * (smem + 1024) > (228u << 10);
+    return rs < 2 && one_cta ? 1024 : 512;
+}
+
 // Every plan raises a kernel's dynamic shared-memory limit to the device
 // maximum (once per kernel and device), so plans of different sizes can
 // coexist; the amount a launch uses is still its own.
@@ -420,7 +428,8 @@ at3r_status run_slab_t(at3r_plan* p, const float* proj, size_t tilt_stride, int 
     TE(p, st, KK_BP_WBP, es * S * (double)T * N + f4 * 4 * vox, 4 * vox * T);
     TB(p, st);
     dispatch_rs(p->f2x.rs, [&](auto R) {
-        k_row_r2c<decltype(R)::value><<<dim3((Nz + p->b_row - 1) / p->b_row, S), 512, p->smem_row, st>>>(
+        k_row_r2c<decltype(R)::value><<<dim3((Nz + p->b_row - 1) / p->b_row, S),
+                                        fft_threads(decltype(R)::value, p->smem_row), p->smem_row, st>>>(
             g2, Nx, Nz, p->f2x.plan, p->b_row, yws);
     });
     TE(p, st, KK_ROW_R2C, f4 * 4 * vox + 8.0 * S * 2 * Nz * KX, 4 * vox);
@@ -428,7 +437,8 @@ at3r_status run_slab_t(at3r_plan* p, const float* proj, size_t tilt_stride, int 
     float2* w = reinterpret_cast<float2*>(g2);
     TB(p, st);
     dispatch_rs(p->rs_zcrop, [&](auto R) {
-        k_zcrop<decltype(R)::value><<<dim3((KX + p->zcrop_cb - 1) / p->zcrop_cb, S), 512, p->smem_zcrop, st>>>(
+        k_zcrop<decltype(R)::value><<<dim3((KX + p->zcrop_cb - 1) / p->zcrop_cb, S),
+                                      fft_threads(decltype(R)::value, p->smem_zcrop), p->smem_zcrop, st>>>(
             yws, Nx, Nz, p->zcrop_cb, p->zcrop_pitch, p->f2z.plan, p->fz.plan, norm, w);
     });
     TE(p, st, KK_ZCROP, 8.0 * S * 3 * Nz * KX, (double)S * 2 * Nz * KX);

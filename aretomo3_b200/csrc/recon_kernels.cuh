@@ -1072,7 +1072,7 @@ __device__ __forceinline__ float bf_hi(uint32_t u) { return __uint_as_float(u & 
 // eight); otherwise (FP32 only) the volume is plain [slices][Nz][Nx].
 // Grid (ceil(N/256), tilts, ceil(slices / fp_slices<VT>())).
 template <typename ST, typename VT, bool GRP>
-__global__ void __launch_bounds__(256, std::is_same<VT, float>::value ? 6 : 1) k_fp_diff(const float* __restrict__ vol, const void* __restrict__ shadow,
+__global__ void __launch_bounds__(256, std::is_same<VT, float>::value ? 6 : 5) k_fp_diff(const float* __restrict__ vol, const void* __restrict__ shadow,
                                                  int Nx, int Nz, int S, const ST* __restrict__ raw,
                                                  ST* __restrict__ diff, const float* __restrict__ scale,
                                                  const float2* __restrict__ cs, int T, int N, int t0,
@@ -1442,8 +1442,18 @@ __device__ __forceinline__ void row_r2c_block(const float* __restrict__ g, int N
     }
 }
 
+// Threads per CTA of the row and column FFT kernels: up to 1024 for the radix
+// sets that fit 64 registers (where a CTA's two buffers fill an SM's shared
+// memory, one CTA of 32 warps in place of 16; two CTAs of 512 otherwise), 512
+// for the generic radices.  The transforms do not depend on the block size.
 template <int RS>
-__global__ void __launch_bounds__(512, RS < 2 ? 2 : 1) k_row_r2c(const float* __restrict__ g, int Nx, int Nz, const __grid_constant__ FftPlan plan, int B,
+__host__ __device__ constexpr int fft_threads_max()
+{
+    return RS < 2 ? 1024 : 512;
+}
+
+template <int RS>
+__global__ void __launch_bounds__(fft_threads_max<RS>(), 1) k_row_r2c(const float* __restrict__ g, int Nx, int Nz, const __grid_constant__ FftPlan plan, int B,
                                                  float2* __restrict__ y)
 {
     row_r2c_block<RS>(g, Nx, Nz, plan, B, y, blockIdx.x, blockIdx.y);
@@ -1496,7 +1506,7 @@ __device__ __forceinline__ void zcrop_block(const float2* __restrict__ y, int Nx
 }
 
 template <int RS>
-__global__ void __launch_bounds__(512, RS < 2 ? 2 : 1) k_zcrop(const float2* __restrict__ y, int Nx, int Nz, int CB, int pitch,
+__global__ void __launch_bounds__(fft_threads_max<RS>(), 1) k_zcrop(const float2* __restrict__ y, int Nx, int Nz, int CB, int pitch,
                                                const __grid_constant__ FftPlan p2, const __grid_constant__ FftPlan p1, float norm, float2* __restrict__ w)
 {
     zcrop_block<RS>(y, Nx, Nz, CB, pitch, p2, p1, norm, w, blockIdx.x, blockIdx.y);
