@@ -1070,7 +1070,9 @@ __device__ __forceinline__ float bf_hi(uint32_t u) { return __uint_as_float(u & 
 // slice-group layout (one float4 load gives a tap of four slices) and the
 // shadow holds eight slices per voxel (one 16-byte load gives a tap of
 // eight); otherwise (FP32 only) the volume is plain [slices][Nz][Nx].
-// Grid (ceil(N/256), tilts, ceil(slices / fp_slices<VT>())).
+// Grid (ceil(N/256), tilts, ceil(slices / fp_slices<VT>())).  Six CTAs per SM
+// with FP32 taps (40 registers), five with the 16-bit shadow (48): the loop
+// waits on L1 and L2, so resident warps are what hides it.
 template <typename ST, typename VT, bool GRP>
 __global__ void __launch_bounds__(256, std::is_same<VT, float>::value ? 6 : 5) k_fp_diff(const float* __restrict__ vol, const void* __restrict__ shadow,
                                                  int Nx, int Nz, int S, const ST* __restrict__ raw,
