@@ -270,3 +270,25 @@ def test_reduced_precision_at_4k_width_vs_oracle(R, storage, tol, mode):
     print(f"4k {mode} {storage}: rel-L2 vs FP64 oracle {err:.3e}")
     assert np.isfinite(out).all()
     assert err < tol
+
+
+@pytest.mark.parametrize("storage", ["f16", "bf16"])
+def test_reduced_precision_wbp_ragged_steep_vs_oracle(R, storage):
+    """WBP in 16-bit storage on a ragged series — a width that fills no
+    back-projection tile (250), an odd thickness (75), tilts to +-70 degrees
+    whose windows reach the detector's edges, and tilts two orders of magnitude
+    apart in brightness — against the FP64 oracle (FP16 within 1e-3; BF16, with
+    its 8-bit mantissa, within 2e-3)."""
+    tilts = np.linspace(-70, 70, 29).astype(np.float32)
+    frames = np.ascontiguousarray(_series(250, 5, tilts, 75, seed=23))
+    frames[3] *= 40.0
+    frames[20] *= 0.4
+    st = R.STORE_F16 if storage == "f16" else R.STORE_BF16
+    out = ours(R, frames, tilts, dict(mode="wbp", vol_z=75), storage=st)
+    plan = R.Plan(250, 5, tilts, 75, method=R.WBP)
+    ref = wbp(frames, tilts, 75, c2r_mode=1 if plan.c2r == R.C2R_PACKED else 0)
+    plan.close()
+    err = rel_l2(out, ref)
+    print(f"ragged WBP {storage}: rel-L2 vs FP64 oracle {err:.3e}")
+    assert np.isfinite(out).all()
+    assert err < (1e-3 if storage == "f16" else 2e-3)
